@@ -1,0 +1,337 @@
+"""Benchmark: stochastic HSGeneral trajectory-steps/s on B200.
+
+Workload (the precision-form configuration): radical pair with 2 electrons and
+12 spin-1/2 nuclei (8 on A, 4 on B), D = 16384, anisotropic hyperfine tensors
+(seed 1), B = 50 uT in a random direction, 1024 trace-sampled trajectories,
+Krylov dimension 20, dt = 0.5 ns, symmetric recombination k = 1/us; bulk
+complex64 with FP64 reductions (Lanczos, expm, yield sums).  Synthetic,
+seeded inputs of the configuration's shapes.
+
+One bench step = `--chunk` time steps of the whole 1024-trajectory block
+(one msgpu_run call).  value = trajectory-steps per second over the K timed
+steps (max over ranks; ranks hold independent trajectory blocks: weak
+scaling, no collective in the data path).  Inputs (the 128 MiB state and the
+2.6 GiB Krylov basis) are larger than L2, so no L2 flush is needed.
+
+--impl reference times the CPU restatement of the reference algorithm
+(oracle/, complex128 Arnoldi as in SpinSpace::KrylovExpmGeneral) on all host
+cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chunk", type=int, default=50, help="time steps per bench step")
+    ap.add_argument("--traj", type=int, default=1024)
+    ap.add_argument("--plain-steps", type=int, default=4, help="time steps of the complex128 comparison run")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
+    """The CPU restatement (complex128 Arnoldi/MGS, per-column Krylov) on a bounded sample."""
+    from oracle import density as den
+    from oracle import pyoracle as orc
+    from molspin_b200 import systems as S
+    F = w.system.trace_samples(sample_traj, w.seed)
+    times = S.time_grid(sample_steps * w.dt, w.dt)
+    obs = [(den.to_csr(den.pair_operator(op, w.system)), rate) for _, op, rate in w.system.observables()]
+    Hc = w.system.hamiltonian_csr()
+    orc.hs_stochastic(Hc, F[:, :threads], times[:2], obs, kappa=w.system.kappa(), krylov=w.krylov,
+                      nthreads=threads)  # warm-up
+    t0 = time.perf_counter()
+    orc.hs_stochastic(Hc, F, times, obs, kappa=w.system.kappa(), krylov=w.krylov, nthreads=threads)
+    el = time.perf_counter() - t0
+    return {"value": sample_traj * sample_steps / el, "unit": "traj-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{sample_traj} trajectories x {sample_steps} steps of the D=16384 m=20 workload "
+                      f"(complex128 Arnoldi, {el:.1f} s)"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from molspin_b200 import systems as S
+    w = S.precision_large(M=args.traj, steps=args.chunk)
+    threads = os.cpu_count() or 1
+    traj = max(threads, 2 * threads)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference(w, threads, 1, threads)
+    vals = []
+    for _ in range(max(1, min(args.steps, 3))):
+        vals.append(cpu_reference(w, traj, 2, threads))
+    v = sum(x["value"] for x in vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": "SSE traj-steps/s (stochastic HSGeneral, Krylov m=20, D=16384)",
+        "value": v, "unit": "traj-steps/s", "n_gpus": world, "steps": len(vals), "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded)",
+        "config": {"workload": w.name, "trajectories": args.traj, "dim": w.system.dim, "krylov": w.krylov},
+        "cpu_baseline": {**vals[-1], "value": v},
+        "e2e": {"value": v, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference binary not buildable here (Armadillo absent): CPU restatement of its algorithm, all cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from molspin_b200 import _lib as L
+    from molspin_b200 import hsgeneral as hs
+    from molspin_b200 import systems as S
+
+    world, rank, local = _dist()
+    M, chunk, K, W = args.traj, args.chunk, args.steps, args.warmup
+    w = S.precision_large(M=M, steps=chunk)
+    sysm = w.system
+    D = sysm.dim
+    rowptr, col, val = sysm.hamiltonian_csr()
+    F = sysm.trace_samples(M, w.seed + rank)
+    obs = [(op, rate) for _, op, rate in sysm.observables()]
+    times = S.time_grid(chunk * w.dt, w.dt)
+    stream = torch.cuda.current_stream()
+
+    p = hs.HSPropagatorB200(local)
+    L.lib.msgpu_set_stream(p.ctx, stream.cuda_stream)
+    p.set_hamiltonian(rowptr, col, val)
+    p.set_reaction(kappa=sysm.kappa())
+    p.set_electron_pair(*sysm.electron_strides())
+    p.set_observables(obs)
+    p.set_factors(F)
+
+    def bench_step(first: bool, k: int):
+        p.propagate(times, w.krylov, "c64", step_offset=k * chunk, accumulate=not first)
+
+    # warm-up
+    for k in range(W):
+        bench_step(k == 0, k)
+    _barrier(world)
+    launches0 = p.launch_count()
+    p.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    ev0.record(stream)
+    for k in range(K):
+        bench_step(False, W + k)
+    ev1.record(stream)
+    _barrier(world)
+    clk = clocks.stop()
+    el_ms = ev0.elapsed_time(ev1)
+    apply_ms, apply_n = p.profile_read(L.KC_APPLY)
+    orth_ms, orth_n = p.profile_read(L.KC_ORTH)
+    comb_ms, comb_n = p.profile_read(L.KC_COMBINE)
+    p.profile(False)
+    launches = p.launch_count() - launches0
+    el_max = _max_over_ranks(el_ms, world)
+    traj_steps = world * M * chunk * K
+    value = traj_steps / (el_max / 1e3)
+
+    # roofline of the dominant kernel (Lanczos SpMM): algorithmic bytes per
+    # launch = read the block's Krylov vector once + write H v once (D*M*8 each)
+    # + the CSR Hamiltonian (nnz * (8 + 4) + 4 (D+1)).
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
+    ldm = (M + 63) // 64 * 64
+    alg_bytes = 2 * D * M * 8 + len(col) * 12 + 4 * (D + 1)
+    apply_avg_s = apply_ms / max(1, apply_n) / 1e3
+    achieved = alg_bytes / apply_avg_s / 1e9 if apply_n else None
+
+    # plain complex128 path (reference-faithful Arnoldi) on a short segment,
+    # and the singlet-yield deviation of the complex64 form from it
+    Fp = F[:, :M]
+    plain_steps = args.plain_steps
+    tp = S.time_grid(plain_steps * w.dt, w.dt)
+    p.set_factors(Fp)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    p.propagate(tp, w.krylov, "c128")  # warm
+    p.set_factors(Fp)
+    t0.record(stream)
+    p.propagate(tp, w.krylov, "c128")
+    t1.record(stream)
+    torch.cuda.synchronize()
+    plain_value = M * plain_steps / (t0.elapsed_time(t1) / 1e3)
+    _, ens128 = p.yields()
+    p.set_factors(Fp)
+    p.propagate(tp, w.krylov, "c64")
+    _, ens64 = p.yields()
+    yerr = abs(ens64[0] - ens128[0]) / abs(ens128[0])
+
+    # end to end through the public API with host buffers: every step uploads
+    # the factor block from pinned host memory, runs, and reads the yields back
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty((M, D), dtype=torch.complex128, pin_memory=True)
+        pinned.numpy()[:] = F.T
+        per = np.zeros((M, len(obs)))
+        ens = np.zeros(len(obs))
+        E = max(1, min(K, 3))
+        _barrier(world)
+        t_0 = time.perf_counter()
+        for k in range(E):
+            rc = L.lib.msgpu_upload_factors(p.ctx, D, M, L.C.cast(pinned.data_ptr(), L.C.POINTER(L.C.c_double)))
+            assert rc == 0, L.lib.msgpu_last_error(p.ctx)
+            p.propagate(times, w.krylov, "c64", step_offset=k * chunk)
+            hs._check(p.ctx, L.lib.msgpu_fetch_yields(p.ctx, L.dptr(per), L.dptr(ens)))
+        _barrier(world)
+        el_e2e = _max_over_ranks(time.perf_counter() - t_0, world)
+        e2e = {"value": world * M * chunk * E / el_e2e, "unit": "traj-steps/s",
+               "h2d_bytes_per_step": D * M * 16, "d2h_bytes_per_step": per.nbytes + ens.nbytes + len(times) * len(obs) * 8,
+               "steps": E}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        cpu = cpu_reference(w, threads, 2, threads)
+
+    p.close()
+    if rank == 0:
+        line = {
+            "metric": "SSE traj-steps/s (stochastic HSGeneral, Krylov m=20, D=16384)",
+            "value": value, "unit": "traj-steps/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": el_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 (FP64 reductions/expm/sums)", "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "trajectories_per_gpu": M, "dim": D, "nnz": int(len(col)),
+                       "krylov": w.krylov, "dt_ns": w.dt, "time_steps_per_bench_step": chunk,
+                       "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos",
+                       "parallelism": f"independent trajectory blocks x{world}"},
+            "roofline": {"bound": "hbm", "kernel": "k_lanczos_apply", "achieved": achieved, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+                         "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_ms": apply_avg_s * 1e3, "launches": apply_n,
+                         "share_of_step": apply_ms / el_ms if el_ms else None},
+            "kernel_ms": {"apply": apply_ms, "update": orth_ms, "combine": comb_ms},
+            "plain_c128": {"value": plain_value, "unit": "traj-steps/s", "steps": plain_steps,
+                           "speedup_of_c64": value / world / plain_value},
+            "yield_rel_err_c64_vs_c128": yerr,
+            "clocks": clk,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/* msgpu.h -- C ABI of the B200 HSGeneral stochastic propagation library.
+ *
+ * This library replaces, for the stochastic static case, the body of the
+ * HSGeneral time loop of MolSpin (RunSection/General/HS/TaskHSGeneral.cpp:
+ * 471-560): per step the observable evaluation
+ * (HSObservableCollector::Evaluate, HSObservableCollector.cpp:276-288), the
+ * symmetric stochastic split (HSPropagator::StepStochastic,
+ * HSPropagator.cpp:131-140) with its fixed-dimension Krylov step
+ * (HSPropagator::Step Krylov branch, HSPropagator.cpp:64-78, i.e.
+ * SpinSpace::KrylovExpmGeneral / ArnoldiProcess,
+ * SpinAPI/SpinSpace/SpinSpace_operators.cpp:1257-1408) and the
+ * singlet-triplet random-unitary noise (SpinAPI::ApplyStochasticRelaxationHilbert,
+ * SpinAPI/SpinSpace/SpinSpace_relaxation.cpp:1211-1254), and afterwards the
+ * trapezoid integration (HSObservableCollector::IntegrateFiniteTime,
+ * HSObservableCollector.cpp:304-326).
+ *
+ * Everything the host side of MolSpin still builds -- the Hamiltonian
+ * (HSHamiltonianBuilder), the Haberkorn operator K (HSReactionRelaxation),
+ * the trace-sampled factors (HSStatePreparation) and the time grid -- is
+ * handed over as plain arrays.  Complex numbers are interleaved (re, im)
+ * doubles.  Every function returns MSGPU_OK (0) or an error code and fills
+ * the context's message (msgpu_last_error), mirroring the reference's
+ * bool + std::string &error convention (e.g. HSPropagator.cpp:51-102).
+ *
+ * Units follow the reference: H in rad/ns, rates in 1/ns, times in ns.
+ */
+#ifndef MSGPU_H
+#define MSGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSGPU_OK 0
+#define MSGPU_ERR_INVALID 1   /* bad argument or missing input */
+#define MSGPU_ERR_BUDGET 2    /* device memory budget of the context exceeded */
+#define MSGPU_ERR_NONFINITE 3 /* a non-finite value appeared on the device */
+#define MSGPU_ERR_EXPM 4      /* small matrix exponential failed (singular Pade denominator) */
+#define MSGPU_ERR_CUDA 6      /* CUDA runtime error */
+#define MSGPU_ERR_STATE 7     /* call out of order (e.g. run before upload) */
+
+/* Precision forms. */
+#define MSGPU_PREC_C128 0 /* plain form: complex128 everywhere (reference parity) */
+#define MSGPU_PREC_C64 1  /* precision form: complex64 vectors and H, FP64 reductions, expm and sums */
+
+/* Krylov recurrences. */
+#define MSGPU_REC_AUTO 0    /* Arnoldi for C128, Lanczos for C64 with scalar K */
+#define MSGPU_REC_ARNOLDI 1 /* Arnoldi on G = -iH - K (as SpinSpace::ArnoldiProcess) */
+#define MSGPU_REC_LANCZOS 2 /* Lanczos on H; valid only when K is a scalar */
+
+/* Propagators. */
+#define MSGPU_PROP_KRYLOV 0
+
+/* Noise modes for the singlet-triplet dephasing Operator. */
+#define MSGPU_NOISE_NONE 0
+#define MSGPU_NOISE_REPLAY 1 /* host-supplied flip bits (e.g. the reference's mt19937 stream) */
+#define MSGPU_NOISE_PHILOX 2 /* on-device Philox4x32-10 keyed by (seed, trajectory, step, half) */
+
+typedef struct msgpu_ctx msgpu_ctx;
+
+typedef struct msgpu_run_params {
+    const double *times;   /* time points t_0 < t_1 < ... (ns); one step per interval */
+    int ntimes;            /* number of time points (steps = ntimes - 1) */
+    int krylov_dim;        /* krylovsize (reference default 16, HSExecutionPlan.h:63); 1..32 */
+    int precision;         /* MSGPU_PREC_* */
+    int recurrence;        /* MSGPU_REC_* */
+    int propagator;        /* MSGPU_PROP_KRYLOV */
+    long long step_offset; /* global index of the first step (noise counters / replay bits) */
+    int accumulate;        /* 0: start new yield integrals at times[0]; 1: continue the previous run */
+} msgpu_run_params;
+
+/* Create a context on CUDA device `device`; all device memory it allocates is
+ * charged against hbm_budget_bytes (0 = no limit).  Returns NULL on failure. */
+msgpu_ctx *msgpu_create(int device, size_t hbm_budget_bytes);
+void msgpu_destroy(msgpu_ctx *ctx);
+const char *msgpu_last_error(const msgpu_ctx *ctx);
+/* Bytes of device memory currently held by the context. */
+size_t msgpu_device_bytes(const msgpu_ctx *ctx);
+
+/* Use an external cudaStream_t (NULL restores the context's own stream). */
+int msgpu_set_stream(msgpu_ctx *ctx, void *cuda_stream);
+
+/* Hamiltonian H (rad/ns) as CSR with int32 indices; val holds nnz complex
+ * values.  Replaces the sp_cx_mat passed to HSPropagator::Step (HSPropagator.h:40-41). */
+int msgpu_upload_hamiltonian_csr(msgpu_ctx *ctx, int dim, const int *rowptr, const int *col, const double *val);
+
+/* K = kappa * I (symmetric recombination: kappa = k/2,
+ * HSReactionRelaxation::BuildReactionForOrientation, HSReactionRelaxation.cpp:134-164). */
+int msgpu_set_reaction_scalar(msgpu_ctx *ctx, double kappa);
+/* General K as CSR (dimension of the uploaded H). */
+int msgpu_upload_reaction_csr(msgpu_ctx *ctx, const int *rowptr, const int *col, const double *val);
+
+/* Kronecker strides of the two spin-1/2 spins of the singlet-triplet pair in
+ * the basis index (index = sum_k digit_k * stride_k, digit 0 = m=+1/2).  The
+ * reference's basis follows the SpinSpace spin order (SpinSpace_management.cpp:37). */
+int msgpu_set_electron_pair(msgpu_ctx *ctx, int stride1, int stride2);
+
+/* Observables O = op (4x4, row-major, pair basis |e1 e2> = uu, ud, du, dd) on
+ * the pair, identity elsewhere; each value is multiplied by `rate`
+ * (transition yields rate * P_source, HSObservableCollector.cpp:101-127).
+ * At most 8. */
+int msgpu_clear_observables(msgpu_ctx *ctx);
+int msgpu_add_pair_observable(msgpu_ctx *ctx, const double *op4x4, double rate);
+
+/* Singlet-triplet dephasing Operator with rate st_rate (1/ns); the random
+ * unitary U = PS - PT is applied with per-half-step probability
+ * -expm1(-st_rate*h)/2 (SpinSpace_relaxation.cpp:1233).  For
+ * MSGPU_NOISE_REPLAY, bits holds one bit per (step, half, trajectory) at
+ * index (step*2 + half)*ntraj + t for nsteps steps. */
+int msgpu_set_st_noise(msgpu_ctx *ctx, double st_rate, int mode, unsigned long long seed,
+                       const unsigned char *bits, long long nsteps, int ntraj);
+
+/* Trajectory block: D x ntraj column-major complex (HSPreparedState factors,
+ * HSStatePreparation.h:31-56, usually already scaled by 1/sqrt(M)). */
+int msgpu_upload_factors(msgpu_ctx *ctx, int dim, int ntraj, const double *factors);
+/* Same, from device memory (interleaved complex128, column-major D x ntraj). */
+int msgpu_upload_factors_device(msgpu_ctx *ctx, int dim, int ntraj, const void *factors_device);
+int msgpu_download_factors(msgpu_ctx *ctx, double *factors);
+
+/* Run the stochastic finite-time loop over params->times (one orientation). */
+int msgpu_run(msgpu_ctx *ctx, const msgpu_run_params *params);
+
+/* Yield integrals so far: per trajectory (ntraj x nobs, trajectory-major) and
+ * ensemble (sum over trajectories, nobs).  Either pointer may be NULL. */
+int msgpu_fetch_yields(msgpu_ctx *ctx, double *per_traj, double *ensemble);
+/* Ensemble observable values at each time point of the last run
+ * ((ntimes) x nobs), the rows of orientationValues in TaskHSGeneral.cpp:470-482. */
+int msgpu_fetch_values(msgpu_ctx *ctx, double *values);
+
+/* Kernel timing with CUDA events on the launch stream.  Classes:
+ * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield. */
+int msgpu_profile_enable(msgpu_ctx *ctx, int enable);
+int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long long *launches);
+
+/* Number of kernels this context launched since creation. */
+long long msgpu_launch_count(const msgpu_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MSGPU_H */

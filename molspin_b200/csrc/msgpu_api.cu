@@ -1,0 +1,840 @@
+// msgpu_api.cu -- C ABI of msgpu (include/msgpu.h): context, uploads and the
+// host-side orchestration of the per-step kernel sequence.
+
+#include "msgpu.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "msgpu_kernels.cuh"
+
+using namespace msgpu;
+
+namespace {
+
+enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_N = 6 };
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct msgpu_ctx {
+    int device = 0;
+    size_t budget = 0;
+    size_t used = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+    long long launches = 0;
+
+    // Hamiltonian
+    int D = 0, nnz = 0;
+    DevBuf hrow, hcol, hval, hhi, hlo;
+    // reaction
+    bool k_scalar = true;
+    double kappa = 0.0;
+    DevBuf krow, kcol, kval;
+    // electron pair
+    int s1 = 0, s2 = 0;
+    bool pair_swapped = false;
+    std::vector<std::array<double, 32>> obs;  // user basis, row-major 4x4 complex
+    std::vector<double> rates;
+    // noise
+    int noise_mode = MSGPU_NOISE_NONE;
+    double st_rate = 0.0;
+    unsigned long long seed = 0;
+    DevBuf bits;
+    long long bits_steps = 0;
+    int bits_ntraj = 0;
+    // state
+    int M = 0, ldm = 0;
+    DevBuf psi128;       // ldm x D interleaved complex128 (plain form state)
+    int state_prec = -1;  // precision holding the current state
+    // workspace
+    int ws_prec = -1, ws_m = 0;
+    DevBuf basis, wbuf, zbuf, ubuf, part, part2, hess, tdiag, toff, coef, mdim, scale, alpha, beta0;
+    DevBuf qpart_obs, qpart_nrm, prev, acc, comp, rates_d, status, values_d;
+    int ntiles = 0, rows_per_tile = 0, qtiles = 0, quartets_per_tile = 0;
+    // yields
+    bool have_integrals = false;
+    std::vector<double> last_values;
+    int last_ntimes = 0;
+    // profiling
+    bool prof = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+    double prof_ms[KC_N] = {0};
+    long long prof_n[KC_N] = {0};
+};
+
+namespace {
+
+int fail(msgpu_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(msgpu_ctx *c, cudaError_t e, const char *what)
+{
+    return fail(c, MSGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void release(msgpu_ctx *c, DevBuf &b)
+{
+    if (b.p) {
+        cudaFree(b.p);
+        c->used -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int ensure(msgpu_ctx *c, DevBuf &b, size_t bytes, const char *what)
+{
+    if (bytes == 0) bytes = 16;
+    if (b.p && b.bytes >= bytes) return MSGPU_OK;
+    release(c, b);
+    if (c->budget && c->used + bytes > c->budget)
+        return fail(c, MSGPU_ERR_BUDGET, std::string("device memory budget exceeded allocating ") + what + " (" +
+                                             std::to_string(bytes) + " bytes, " + std::to_string(c->used) +
+                                             " in use, budget " + std::to_string(c->budget) + ")");
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return cuda_fail(c, e, what);
+    }
+    b.bytes = bytes;
+    c->used += bytes;
+    return MSGPU_OK;
+}
+
+int device_guard(msgpu_ctx *c)
+{
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    return MSGPU_OK;
+}
+
+struct Timed {
+    msgpu_ctx *c;
+    int cls;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timed(msgpu_ctx *c_, int cls_) : c(c_), cls(cls_)
+    {
+        ++c->launches;
+        if (!c->prof) return;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, c->stream);
+    }
+    ~Timed()
+    {
+        if (!c->prof) return;
+        cudaEventRecord(b, c->stream);
+        c->ev.push_back({cls, {a, b}});
+    }
+};
+
+void collect_profile(msgpu_ctx *c)
+{
+    for (auto &e : c->ev) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.second.first, e.second.second);
+        c->prof_ms[e.first] += ms;
+        c->prof_n[e.first] += 1;
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    c->ev.clear();
+}
+
+inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+// Rows per tile: keep about 64-128 row tiles per trajectory tile so that the
+// partial-sum buffers stay small and every SM has several CTAs.
+int pick_rows_per_tile(int D)
+{
+    int R = D / 64;
+    R = std::max(8, std::min(512, R));
+    R = (R + 7) / 8 * 8;
+    return R;
+}
+
+PairObs make_pair_obs(const msgpu_ctx *c)
+{
+    PairObs po;
+    std::memset(&po, 0, sizeof(po));
+    po.nobs = static_cast<int>(c->obs.size());
+    // kernel pair basis index = 2*digit(stride s1) + digit(stride s2); when the
+    // user's first electron has the smaller stride the roles swap (1 <-> 2).
+    const int perm[4] = {0, 2, 1, 3};
+    for (int o = 0; o < po.nobs; ++o)
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const int ua = c->pair_swapped ? perm[a] : a, ub = c->pair_swapped ? perm[b] : b;
+                po.op[o][a * 4 + b] = make_double2(c->obs[o][2 * (ua * 4 + ub)], c->obs[o][2 * (ua * 4 + ub) + 1]);
+            }
+    return po;
+}
+
+}  // namespace
+
+extern "C" {
+
+msgpu_ctx *msgpu_create(int device, size_t hbm_budget_bytes)
+{
+    auto *c = new msgpu_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    c->stream = c->own;
+    return c;
+}
+
+void msgpu_destroy(msgpu_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    collect_profile(c);
+    DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->krow, &c->kcol, &c->kval, &c->bits,
+                     &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
+                     &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
+                     &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d};
+    for (DevBuf *b : all) release(c, *b);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+const char *msgpu_last_error(const msgpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+size_t msgpu_device_bytes(const msgpu_ctx *c) { return c ? c->used : 0; }
+
+long long msgpu_launch_count(const msgpu_ctx *c) { return c ? c->launches : 0; }
+
+int msgpu_set_stream(msgpu_ctx *c, void *s)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    c->stream = s ? static_cast<cudaStream_t>(s) : c->own;
+    return MSGPU_OK;
+}
+
+int msgpu_upload_hamiltonian_csr(msgpu_ctx *c, int dim, const int *rowptr, const int *col, const double *val)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (dim < 4 || !rowptr || !col || !val) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian: dimension >= 4 and CSR arrays required");
+    if (int rc = device_guard(c)) return rc;
+    const int nnz = rowptr[dim];
+    if (rowptr[0] != 0 || nnz < 0) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian: malformed row pointer");
+    for (int r = 0; r < dim; ++r)
+        if (rowptr[r + 1] < rowptr[r]) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian: row pointer not monotone");
+    std::vector<float> hi(2 * static_cast<size_t>(nnz)), lo(2 * static_cast<size_t>(nnz));
+    for (int k = 0; k < nnz; ++k) {
+        if (col[k] < 0 || col[k] >= dim) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian: column index out of range");
+        for (int p = 0; p < 2; ++p) {
+            const double v = val[2 * k + p];
+            if (!std::isfinite(v)) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian: non-finite value");
+            const float h = static_cast<float>(v);
+            hi[2 * k + p] = h;
+            lo[2 * k + p] = static_cast<float>(v - static_cast<double>(h));
+        }
+    }
+    if (c->D != 0 && c->D != dim) {
+        // dimension change invalidates state and reaction operator
+        c->state_prec = -1;
+        c->M = 0;
+        c->k_scalar = true;
+    }
+    int rc;
+    if ((rc = ensure(c, c->hrow, sizeof(int) * (dim + 1), "H rowptr")) ||
+        (rc = ensure(c, c->hcol, sizeof(int) * std::max(1, nnz), "H col")) ||
+        (rc = ensure(c, c->hval, sizeof(double2) * std::max(1, nnz), "H val")) ||
+        (rc = ensure(c, c->hhi, sizeof(float2) * std::max(1, nnz), "H hi")) ||
+        (rc = ensure(c, c->hlo, sizeof(float2) * std::max(1, nnz), "H lo")))
+        return rc;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->hrow.p, rowptr, sizeof(int) * (dim + 1), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->hcol.p, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->hval.p, val, sizeof(double2) * nnz, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->hhi.p, hi.data(), sizeof(float2) * nnz, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->hlo.p, lo.data(), sizeof(float2) * nnz, cudaMemcpyHostToDevice, c->stream)))
+        return cuda_fail(c, e, "Hamiltonian upload");
+    if ((e = cudaStreamSynchronize(c->stream))) return cuda_fail(c, e, "Hamiltonian upload");
+    c->D = dim;
+    c->nnz = nnz;
+    return MSGPU_OK;
+}
+
+int msgpu_set_reaction_scalar(msgpu_ctx *c, double kappa)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!std::isfinite(kappa)) return fail(c, MSGPU_ERR_NONFINITE, "reaction: non-finite kappa");
+    c->k_scalar = true;
+    c->kappa = kappa;
+    return MSGPU_OK;
+}
+
+int msgpu_upload_reaction_csr(msgpu_ctx *c, const int *rowptr, const int *col, const double *val)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (c->D == 0) return fail(c, MSGPU_ERR_STATE, "reaction: upload the Hamiltonian first");
+    if (!rowptr || !col || !val) return fail(c, MSGPU_ERR_INVALID, "reaction: CSR arrays required");
+    if (int rc = device_guard(c)) return rc;
+    const int D = c->D, nnz = rowptr[D];
+    if (rowptr[0] != 0 || nnz < 0) return fail(c, MSGPU_ERR_INVALID, "reaction: malformed row pointer");
+    for (int r = 0; r < D; ++r)
+        if (rowptr[r + 1] < rowptr[r]) return fail(c, MSGPU_ERR_INVALID, "reaction: row pointer not monotone");
+    for (int k = 0; k < nnz; ++k) {
+        if (col[k] < 0 || col[k] >= D) return fail(c, MSGPU_ERR_INVALID, "reaction: column index out of range");
+        if (!std::isfinite(val[2 * k]) || !std::isfinite(val[2 * k + 1]))
+            return fail(c, MSGPU_ERR_NONFINITE, "reaction: non-finite value");
+    }
+    int rc;
+    if ((rc = ensure(c, c->krow, sizeof(int) * (D + 1), "K rowptr")) ||
+        (rc = ensure(c, c->kcol, sizeof(int) * std::max(1, nnz), "K col")) ||
+        (rc = ensure(c, c->kval, sizeof(double2) * std::max(1, nnz), "K val")))
+        return rc;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->krow.p, rowptr, sizeof(int) * (D + 1), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->kcol.p, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->kval.p, val, sizeof(double2) * nnz, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "reaction upload");
+    c->k_scalar = false;
+    return MSGPU_OK;
+}
+
+int msgpu_set_electron_pair(msgpu_ctx *c, int stride1, int stride2)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (stride1 <= 0 || stride2 <= 0 || stride1 == stride2)
+        return fail(c, MSGPU_ERR_INVALID, "electron pair: two distinct positive strides required");
+    const int hi = std::max(stride1, stride2), lo = std::min(stride1, stride2);
+    if (hi % (2 * lo) != 0)
+        return fail(c, MSGPU_ERR_INVALID, "electron pair: strides must belong to two spin-1/2 digits of the product basis");
+    if (c->D && (c->D % (2 * hi) != 0))
+        return fail(c, MSGPU_ERR_INVALID, "electron pair: strides inconsistent with the Hilbert dimension");
+    c->s1 = hi;
+    c->s2 = lo;
+    c->pair_swapped = stride1 < stride2;
+    return MSGPU_OK;
+}
+
+int msgpu_clear_observables(msgpu_ctx *c)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    c->obs.clear();
+    c->rates.clear();
+    c->have_integrals = false;
+    return MSGPU_OK;
+}
+
+int msgpu_add_pair_observable(msgpu_ctx *c, const double *op, double rate)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!op || !std::isfinite(rate)) return fail(c, MSGPU_ERR_INVALID, "observable: operator and finite rate required");
+    if (c->obs.size() >= 8) return fail(c, MSGPU_ERR_INVALID, "observable: at most 8 pair observables");
+    std::array<double, 32> a;
+    for (int i = 0; i < 32; ++i) {
+        if (!std::isfinite(op[i])) return fail(c, MSGPU_ERR_NONFINITE, "observable: non-finite entry");
+        a[i] = op[i];
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            const double dr = a[2 * (i * 4 + j)] - a[2 * (j * 4 + i)];
+            const double di = a[2 * (i * 4 + j) + 1] + a[2 * (j * 4 + i) + 1];
+            if (std::abs(dr) > 1e-12 || std::abs(di) > 1e-12)
+                return fail(c, MSGPU_ERR_INVALID, "observable: operator must be Hermitian");
+        }
+    c->obs.push_back(a);
+    c->rates.push_back(rate);
+    c->have_integrals = false;
+    return MSGPU_OK;
+}
+
+int msgpu_set_st_noise(msgpu_ctx *c, double st_rate, int mode, unsigned long long seed, const unsigned char *bits,
+                       long long nsteps, int ntraj)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!std::isfinite(st_rate) || st_rate < 0.0) return fail(c, MSGPU_ERR_INVALID, "noise: rate must be finite and >= 0");
+    if (mode < MSGPU_NOISE_NONE || mode > MSGPU_NOISE_PHILOX) return fail(c, MSGPU_ERR_INVALID, "noise: unknown mode");
+    if (int rc = device_guard(c)) return rc;
+    c->noise_mode = (st_rate > 0.0) ? mode : MSGPU_NOISE_NONE;
+    c->st_rate = st_rate;
+    c->seed = seed;
+    if (c->noise_mode == MSGPU_NOISE_REPLAY) {
+        if (!bits || nsteps <= 0 || ntraj <= 0) return fail(c, MSGPU_ERR_INVALID, "noise: replay bits required");
+        const size_t bytes = static_cast<size_t>((nsteps * 2 * ntraj + 7) / 8);
+        if (int rc = ensure(c, c->bits, bytes, "noise bits")) return rc;
+        cudaError_t e;
+        if ((e = cudaMemcpyAsync(c->bits.p, bits, bytes, cudaMemcpyHostToDevice, c->stream)) ||
+            (e = cudaStreamSynchronize(c->stream)))
+            return cuda_fail(c, e, "noise bits upload");
+        c->bits_steps = nsteps;
+        c->bits_ntraj = ntraj;
+    }
+    return MSGPU_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int upload_factors_impl(msgpu_ctx *c, int dim, int ntraj, const void *src, cudaMemcpyKind kind)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (c->D == 0) return fail(c, MSGPU_ERR_STATE, "factors: upload the Hamiltonian first");
+    if (dim != c->D) return fail(c, MSGPU_ERR_INVALID, "factors: dimension differs from the Hamiltonian");
+    if (ntraj <= 0 || !src) return fail(c, MSGPU_ERR_INVALID, "factors: at least one trajectory required");
+    if (int rc = device_guard(c)) return rc;
+    const int ldm = (ntraj + 63) / 64 * 64;
+    const size_t n = static_cast<size_t>(dim) * ldm;
+    if (int rc = ensure(c, c->psi128, n * sizeof(double2), "state")) return rc;
+    // staging copy in column-major order, then a tiled transpose on the device;
+    // the staging area is the Krylov workspace when it is large enough.
+    const size_t sbytes = static_cast<size_t>(dim) * ntraj * sizeof(double2);
+    if (int rc = ensure(c, c->zbuf, sbytes, "upload staging")) return rc;
+    cudaError_t e = cudaMemcpyAsync(c->zbuf.p, src, sbytes, kind, c->stream);
+    if (e) return cuda_fail(c, e, "factors upload");
+    dim3 grid(ceil_div(dim, 32), ldm / 32), block(32, 8);
+    {
+        Timed tm(c, KC_COMBINE);
+        k_cols_to_interleaved<double2><<<grid, block, 0, c->stream>>>(static_cast<double2 *>(c->psi128.p),
+                                                                      static_cast<const double2 *>(c->zbuf.p), dim,
+                                                                      ntraj, ldm);
+    }
+    if ((e = cudaGetLastError())) return cuda_fail(c, e, "factors transpose");
+    if ((e = cudaStreamSynchronize(c->stream))) return cuda_fail(c, e, "factors upload");
+    if (c->M != ntraj) c->ws_prec = -1;
+    c->M = ntraj;
+    c->ldm = ldm;
+    c->state_prec = MSGPU_PREC_C128;
+    c->have_integrals = false;
+    return MSGPU_OK;
+}
+
+// Workspace for (precision, Krylov dimension m) at the current (D, ldm).
+int ensure_workspace(msgpu_ctx *c, int prec, int m)
+{
+    const int D = c->D, ldm = c->ldm, nobs = std::max<int>(1, static_cast<int>(c->obs.size()));
+    const size_t n = static_cast<size_t>(D) * ldm;
+    c->rows_per_tile = pick_rows_per_tile(D);
+    c->ntiles = ceil_div(D, c->rows_per_tile);
+    const int Q = D / 4;
+    c->quartets_per_tile = std::max(8, std::min(256, Q / 64));
+    c->qtiles = ceil_div(Q, c->quartets_per_tile);
+    int rc;
+    if (prec == MSGPU_PREC_C128) {
+        // basis V_0..V_{m-1}; W/Z ping-pong
+        if ((rc = ensure(c, c->basis, n * m * sizeof(double2), "Krylov basis")) ||
+            (rc = ensure(c, c->wbuf, n * sizeof(double2), "Krylov W")) ||
+            (rc = ensure(c, c->zbuf, n * sizeof(double2), "Krylov Z")) ||
+            (rc = ensure(c, c->part, static_cast<size_t>(c->ntiles) * (m + 1) * ldm * sizeof(double2), "partials")) ||
+            (rc = ensure(c, c->part2, static_cast<size_t>(3) * (m + 1) * ldm * sizeof(double2), "dots")) ||
+            (rc = ensure(c, c->hess, static_cast<size_t>(ldm) * m * m * sizeof(double2), "Hessenberg")))
+            return rc;
+    } else {
+        // w_0 (= state) .. w_m, and U
+        if ((rc = ensure(c, c->basis, n * (m + 1) * sizeof(float2), "Lanczos basis")) ||
+            (rc = ensure(c, c->ubuf, n * sizeof(float2), "Lanczos U")) ||
+            (rc = ensure(c, c->part, static_cast<size_t>(c->ntiles) * ldm * sizeof(double), "partials")) ||
+            (rc = ensure(c, c->tdiag, static_cast<size_t>(ldm) * m * sizeof(double), "T diagonal")) ||
+            (rc = ensure(c, c->toff, static_cast<size_t>(ldm) * m * sizeof(double), "T offdiagonal")) ||
+            (rc = ensure(c, c->alpha, static_cast<size_t>(ldm) * sizeof(double), "alpha")))
+            return rc;
+    }
+    if ((rc = ensure(c, c->coef, static_cast<size_t>(ldm) * m * sizeof(double2), "coefficients")) ||
+        (rc = ensure(c, c->mdim, static_cast<size_t>(ldm) * sizeof(int), "Krylov dims")) ||
+        (rc = ensure(c, c->scale, static_cast<size_t>(ldm) * (m + 1) * sizeof(double), "scales")) ||
+        (rc = ensure(c, c->beta0, static_cast<size_t>(ldm) * sizeof(double), "beta0")) ||
+        (rc = ensure(c, c->qpart_obs, static_cast<size_t>(c->qtiles) * nobs * ldm * sizeof(double), "obs partials")) ||
+        (rc = ensure(c, c->qpart_nrm, static_cast<size_t>(c->qtiles) * ldm * sizeof(double), "norm partials")) ||
+        (rc = ensure(c, c->prev, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield prev")) ||
+        (rc = ensure(c, c->acc, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield acc")) ||
+        (rc = ensure(c, c->comp, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield comp")) ||
+        (rc = ensure(c, c->rates_d, 8 * sizeof(double), "rates")) ||
+        (rc = ensure(c, c->status, sizeof(int), "status")))
+        return rc;
+    c->ws_prec = prec;
+    c->ws_m = m;
+    return MSGPU_OK;
+}
+
+// Bring the state into the precision of the run.  The complex64 state lives
+// in slot 0 of the Lanczos basis.
+int ensure_state(msgpu_ctx *c, int prec)
+{
+    if (c->state_prec == prec) return MSGPU_OK;
+    const size_t n = static_cast<size_t>(c->D) * c->ldm;
+    const int threads = 256;
+    const int blocks = ceil_div(static_cast<long long>(n), threads);
+    if (prec == MSGPU_PREC_C64 && c->state_prec == MSGPU_PREC_C128) {
+        Timed tm(c, KC_COMBINE);
+        k_convert<float2, double2><<<blocks, threads, 0, c->stream>>>(static_cast<float2 *>(c->basis.p),
+                                                                      static_cast<const double2 *>(c->psi128.p), n);
+    } else if (prec == MSGPU_PREC_C128 && c->state_prec == MSGPU_PREC_C64) {
+        // the c64 basis may have been released by a workspace switch; keep it
+        // alive by converting before any reallocation (see msgpu_run)
+        Timed tm(c, KC_COMBINE);
+        k_convert<double2, float2><<<blocks, threads, 0, c->stream>>>(static_cast<double2 *>(c->psi128.p),
+                                                                      static_cast<const float2 *>(c->basis.p), n);
+    } else {
+        return fail(c, MSGPU_ERR_STATE, "no trajectory state uploaded");
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e) return cuda_fail(c, e, "state conversion");
+    c->state_prec = prec;
+    return MSGPU_OK;
+}
+
+double flip_p(double st_rate, double h) { return -0.5 * std::expm1(-2.0 * (0.5 * st_rate) * h); }
+
+}  // namespace
+
+extern "C" {
+
+int msgpu_upload_factors(msgpu_ctx *c, int dim, int ntraj, const double *factors)
+{
+    return upload_factors_impl(c, dim, ntraj, factors, cudaMemcpyHostToDevice);
+}
+
+int msgpu_upload_factors_device(msgpu_ctx *c, int dim, int ntraj, const void *factors)
+{
+    return upload_factors_impl(c, dim, ntraj, factors, cudaMemcpyDeviceToDevice);
+}
+
+int msgpu_download_factors(msgpu_ctx *c, double *factors)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (c->state_prec < 0 || !factors) return fail(c, MSGPU_ERR_STATE, "no trajectory state to download");
+    if (int rc = device_guard(c)) return rc;
+    const size_t sbytes = static_cast<size_t>(c->D) * c->M * sizeof(double2);
+    if (c->state_prec == MSGPU_PREC_C128 && c->ws_prec != MSGPU_PREC_C128) {
+        if (int rc = ensure(c, c->zbuf, sbytes, "download staging")) return rc;
+    }
+    if (c->zbuf.bytes < sbytes) {
+        if (int rc = ensure(c, c->zbuf, sbytes, "download staging")) return rc;
+    }
+    dim3 grid(ceil_div(c->D, 32), c->ldm / 32), block(32, 8);
+    {
+        Timed tm(c, KC_COMBINE);
+        if (c->state_prec == MSGPU_PREC_C128)
+            k_interleaved_to_cols<double2><<<grid, block, 0, c->stream>>>(
+                static_cast<double2 *>(c->zbuf.p), static_cast<const double2 *>(c->psi128.p), c->D, c->M, c->ldm);
+        else
+            k_interleaved_to_cols<float2><<<grid, block, 0, c->stream>>>(
+                static_cast<double2 *>(c->zbuf.p), static_cast<const float2 *>(c->basis.p), c->D, c->M, c->ldm);
+    }
+    cudaError_t e;
+    if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(factors, c->zbuf.p, sbytes, cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "factors download");
+    return MSGPU_OK;
+}
+
+int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!p || !p->times || p->ntimes < 1) return fail(c, MSGPU_ERR_INVALID, "run: a time grid with at least one point is required");
+    if (c->D == 0) return fail(c, MSGPU_ERR_STATE, "run: no Hamiltonian uploaded");
+    if (c->state_prec < 0) return fail(c, MSGPU_ERR_STATE, "run: no trajectory factors uploaded");
+    if (c->s1 == 0) return fail(c, MSGPU_ERR_STATE, "run: electron pair strides not set");
+    if (c->D % (2 * c->s1) != 0) return fail(c, MSGPU_ERR_INVALID, "run: electron strides inconsistent with the Hilbert dimension");
+    if (c->obs.empty()) return fail(c, MSGPU_ERR_STATE, "run: no observables");
+    if (p->precision != MSGPU_PREC_C128 && p->precision != MSGPU_PREC_C64)
+        return fail(c, MSGPU_ERR_INVALID, "run: unknown precision");
+    if (p->propagator != MSGPU_PROP_KRYLOV) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
+    if (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov)
+        return fail(c, MSGPU_ERR_INVALID, "run: krylov_dim must be in 1..32");
+    for (int s = 0; s < p->ntimes; ++s)
+        if (!std::isfinite(p->times[s]) || (s > 0 && !(p->times[s] > p->times[s - 1])))
+            return fail(c, MSGPU_ERR_INVALID, "run: times must be finite and strictly increasing");
+    int rec = p->recurrence;
+    if (rec == MSGPU_REC_AUTO) rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
+    if (rec == MSGPU_REC_LANCZOS && !c->k_scalar)
+        return fail(c, MSGPU_ERR_INVALID, "run: Lanczos requires a scalar reaction operator K");
+    if (p->precision == MSGPU_PREC_C64 && rec != MSGPU_REC_LANCZOS)
+        return fail(c, MSGPU_ERR_INVALID, "run: the complex64 form implements the Lanczos recurrence only");
+    if (p->precision == MSGPU_PREC_C128 && rec != MSGPU_REC_ARNOLDI)
+        return fail(c, MSGPU_ERR_INVALID, "run: the complex128 form implements the Arnoldi recurrence only");
+    if (c->noise_mode == MSGPU_NOISE_REPLAY) {
+        if (c->bits_ntraj != c->M) return fail(c, MSGPU_ERR_INVALID, "run: replay bits cover a different trajectory count");
+        if (p->step_offset < 0 || p->step_offset + (p->ntimes - 1) > c->bits_steps)
+            return fail(c, MSGPU_ERR_INVALID, "run: replay bits do not cover the requested steps");
+    }
+    if (p->accumulate && !c->have_integrals) return fail(c, MSGPU_ERR_STATE, "run: nothing to continue (accumulate=1)");
+    if (int rc = device_guard(c)) return rc;
+
+    const int D = c->D, ldm = c->ldm, M = c->M;
+    const int m = std::min(p->krylov_dim, D);
+    const int prec = p->precision;
+    const int nobs = static_cast<int>(c->obs.size());
+    const size_t n = static_cast<size_t>(D) * ldm;
+    // The complex64 state lives in slot 0 of the Lanczos basis: park it in the
+    // complex128 state before that buffer is reused or reallocated.
+    if (c->state_prec == MSGPU_PREC_C64) {
+        const size_t need = n * (m + 1) * sizeof(float2);
+        if (prec != MSGPU_PREC_C64 || c->basis.bytes < need)
+            if (int rc = ensure_state(c, MSGPU_PREC_C128)) return rc;
+    }
+    if (int rc = ensure_workspace(c, prec, m)) return rc;
+    if (int rc = ensure_state(c, prec)) return rc;
+    const int mws = m;  // layout stride of the per-trajectory Krylov arrays
+    cudaError_t e;
+    cudaStream_t st = c->stream;
+    if ((e = cudaMemcpyAsync(c->rates_d.p, c->rates.data(), nobs * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemsetAsync(c->status.p, 0, sizeof(int), st)))
+        return cuda_fail(c, e, "run setup");
+    if (!p->accumulate) {
+        if ((e = cudaMemsetAsync(c->acc.p, 0, static_cast<size_t>(nobs) * ldm * sizeof(double), st)) ||
+            (e = cudaMemsetAsync(c->comp.p, 0, static_cast<size_t>(nobs) * ldm * sizeof(double), st)))
+            return cuda_fail(c, e, "run setup");
+    }
+    if (int rc = ensure(c, c->values_d, static_cast<size_t>(p->ntimes) * nobs * sizeof(double), "values")) return rc;
+
+    const PairObs po = make_pair_obs(c);
+    Noise nz;
+    nz.mode = c->noise_mode;
+    nz.bits = static_cast<const uint8_t *>(c->bits.p);
+    nz.bits_steps = c->bits_steps;
+    nz.M = c->noise_mode == MSGPU_NOISE_REPLAY ? c->bits_ntraj : M;
+    nz.seed = c->seed;
+    nz.traj_offset = 0;
+    nz.p_full = 0.0;
+    const int steps = p->ntimes - 1;
+    const long long g0 = p->step_offset;
+    auto pstep = [&](int s) { return s < steps ? flip_p(c->st_rate, 0.5 * (p->times[s + 1] - p->times[s])) : 0.0; };
+
+    const int Q = D / 4, QR = c->quartets_per_tile, qt = c->qtiles;
+    dim3 qgrid(qt, ldm / 32), qblock(32, 8);
+    double *values = static_cast<double *>(c->values_d.p);
+    double *sc = static_cast<double *>(c->scale.p);  // [m+1][ldm]; slot 0 = 1/|psi|
+    double *beta0 = static_cast<double *>(c->beta0.p);
+    auto yield_update = [&](double dt, int init, int row) {
+        Timed tm(c, KC_YIELD);
+        k_yield_update<<<1, 1024, 0, st>>>(static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p),
+                                           qt, nobs, ldm, M, static_cast<double *>(c->rates_d.p), dt, init,
+                                           static_cast<double *>(c->prev.p), static_cast<double *>(c->acc.p),
+                                           static_cast<double *>(c->comp.p), beta0, sc, values + static_cast<size_t>(row) * nobs,
+                                           static_cast<int *>(c->status.p));
+    };
+
+    // Evaluate the first time point and apply the first half-step flip.
+    {
+        Timed tm(c, KC_COMBINE);
+        const long long sB = -1;
+        if (prec == MSGPU_PREC_C128)
+            k_combine<double2, false><<<qgrid, qblock, 0, st>>>(
+                static_cast<double2 *>(c->psi128.p), nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz,
+                steps > 0 ? g0 : -1, 0, pstep(0), sB, 0, 0.0, po, static_cast<double *>(c->qpart_obs.p),
+                static_cast<double *>(c->qpart_nrm.p));
+        else
+            k_combine<float2, false><<<qgrid, qblock, 0, st>>>(
+                static_cast<float2 *>(c->basis.p), nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz,
+                steps > 0 ? g0 : -1, 0, pstep(0), sB, 0, 0.0, po, static_cast<double *>(c->qpart_obs.p),
+                static_cast<double *>(c->qpart_nrm.p));
+    }
+    yield_update(0.0, 1, 0);
+
+    const int R = c->rows_per_tile, nt = c->ntiles;
+    CsrD Hd{static_cast<const int *>(c->hrow.p), static_cast<const int *>(c->hcol.p), static_cast<const double2 *>(c->hval.p)};
+    CsrD Kd{c->k_scalar ? nullptr : static_cast<const int *>(c->krow.p), static_cast<const int *>(c->kcol.p),
+            static_cast<const double2 *>(c->kval.p)};
+    CsrF Hf{static_cast<const int *>(c->hrow.p), static_cast<const int *>(c->hcol.p), static_cast<const float2 *>(c->hhi.p),
+            nullptr};
+    const double kappa = c->k_scalar ? c->kappa : 0.0;
+    const size_t expm_smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
+    const int expm_warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / expm_smem_warp)));
+    if ((e = cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(expm_warps * expm_smem_warp))))
+        return cuda_fail(c, e, "expm shared memory");
+
+    for (int s = 0; s < steps; ++s) {
+        const double dt = p->times[s + 1] - p->times[s];
+        const long long g = g0 + s;
+        if ((e = cudaMemsetAsync(c->mdim.p, 0, ldm * sizeof(int), st))) return cuda_fail(c, e, "mdim reset");
+        if (prec == MSGPU_PREC_C128) {
+            double2 *V = static_cast<double2 *>(c->basis.p);
+            double2 *bufA = static_cast<double2 *>(c->wbuf.p), *bufB = static_cast<double2 *>(c->zbuf.p);
+            double2 *dots = static_cast<double2 *>(c->part2.p);  // [3][m+1][ldm]: h1, h2, norm
+            double2 *h1 = dots, *h2 = dots + static_cast<size_t>(m + 1) * ldm, *nr = dots + 2 * static_cast<size_t>(m + 1) * ldm;
+            const double2 *src = static_cast<const double2 *>(c->psi128.p);
+            double2 *W = bufA;
+            dim3 grid(nt, ldm / 32);
+            for (int j = 0; j < m; ++j) {
+                {
+                    Timed tm(c, KC_APPLY);
+                    k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, V,
+                                                               n, j, static_cast<double2 *>(c->part.p), D, ldm, R);
+                }
+                {
+                    Timed tm(c, KC_REDUCE);
+                    k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(
+                        static_cast<double2 *>(c->part.p), nt, j + 1, ldm, h1);
+                }
+                {
+                    Timed tm(c, KC_ORTH);
+                    k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h1, static_cast<double2 *>(c->part.p), 1, D, ldm, R);
+                }
+                {
+                    Timed tm(c, KC_REDUCE);
+                    k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(
+                        static_cast<double2 *>(c->part.p), nt, j + 1, ldm, h2);
+                }
+                {
+                    Timed tm(c, KC_ORTH);
+                    k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h2, static_cast<double2 *>(c->part.p), 2, D, ldm, R);
+                }
+                {
+                    Timed tm(c, KC_REDUCE);
+                    k_reduce_partials<<<ceil_div(ldm, 256), 256, 0, st>>>(static_cast<double2 *>(c->part.p), nt, 1, ldm, nr);
+                    k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(h1, h2, nr, j, mws, ldm,
+                                                                           static_cast<double2 *>(c->hess.p),
+                                                                           static_cast<int *>(c->mdim.p), sc + ldm);
+                }
+                // next iteration reads W scaled by 1/beta; write into the other buffer
+                src = W;
+                W = (W == bufA) ? bufB : bufA;
+            }
+            {
+                Timed tm(c, KC_EXPM);
+                k_krylov_expm<<<ceil_div(ldm, expm_warps), 32 * expm_warps, expm_warps * expm_smem_warp, st>>>(
+                    static_cast<double2 *>(c->hess.p), nullptr, nullptr, 0.0, static_cast<int *>(c->mdim.p), beta0,
+                    nullptr, mws, ldm, M, dt, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->status.p));
+            }
+            {
+                Timed tm(c, KC_COMBINE);
+                k_combine<double2, true><<<qgrid, qblock, 0, st>>>(
+                    static_cast<double2 *>(c->psi128.p), V, n, static_cast<double2 *>(c->coef.p),
+                    static_cast<int *>(c->mdim.p), mws, c->s1, c->s2, Q, ldm, QR, nz, g, 1, pstep(s),
+                    s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, static_cast<double *>(c->qpart_obs.p),
+                    static_cast<double *>(c->qpart_nrm.p));
+            }
+        } else {
+            float2 *Wb = static_cast<float2 *>(c->basis.p);  // w_0 = state
+            float2 *U = static_cast<float2 *>(c->ubuf.p);
+            double *part = static_cast<double *>(c->part.p);
+            double *alpha = static_cast<double *>(c->alpha.p);
+            double *td = static_cast<double *>(c->tdiag.p), *to = static_cast<double *>(c->toff.p);
+            dim3 grid(nt, ldm / 64);
+            for (int j = 0; j < m; ++j) {
+                {
+                    Timed tm(c, KC_APPLY);
+                    k_lanczos_apply<false><<<grid, kThreads, 0, st>>>(Hf, Wb + j * n, sc + static_cast<size_t>(j) * ldm, U,
+                                                                     part, D, ldm, R);
+                }
+                {
+                    Timed tm(c, KC_REDUCE);
+                    k_lanczos_reduce<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, ldm, 0, j, mws, alpha, td, to,
+                                                                         static_cast<int *>(c->mdim.p));
+                }
+                if (j == m - 1) break;  // T_m is complete; w_m is never used
+                {
+                    Timed tm(c, KC_ORTH);
+                    k_lanczos_update<<<grid, kThreads, 0, st>>>(
+                        U, Wb + j * n, j > 0 ? Wb + (j - 1) * n : nullptr, sc + static_cast<size_t>(j) * ldm,
+                        j > 0 ? sc + static_cast<size_t>(j - 1) * ldm : nullptr, alpha, Wb + (j + 1) * n, part, D, ldm, R);
+                }
+                {
+                    Timed tm(c, KC_REDUCE);
+                    k_lanczos_reduce<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, ldm, 1, j, mws,
+                                                                         sc + static_cast<size_t>(j + 1) * ldm, td, to,
+                                                                         static_cast<int *>(c->mdim.p));
+                }
+            }
+            {
+                Timed tm(c, KC_EXPM);
+                k_krylov_expm<<<ceil_div(ldm, expm_warps), 32 * expm_warps, expm_warps * expm_smem_warp, st>>>(
+                    nullptr, td, to, kappa, static_cast<int *>(c->mdim.p), beta0, sc, mws, ldm, M, dt,
+                    static_cast<double2 *>(c->coef.p), static_cast<int *>(c->status.p));
+            }
+            {
+                Timed tm(c, KC_COMBINE);
+                k_combine<float2, true><<<qgrid, qblock, 0, st>>>(
+                    Wb, Wb, n, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->mdim.p), mws, c->s1, c->s2, Q,
+                    ldm, QR, nz, g, 1, pstep(s), s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po,
+                    static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p));
+            }
+        }
+        yield_update(dt, 0, s + 1);
+        if ((e = cudaGetLastError())) return cuda_fail(c, e, "step launch");
+    }
+    int status = 0;
+    c->last_values.assign(static_cast<size_t>(p->ntimes) * nobs, 0.0);
+    if ((e = cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(c->last_values.data(), values, c->last_values.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+        return cuda_fail(c, e, "run");
+    collect_profile(c);
+    c->last_ntimes = p->ntimes;
+    c->have_integrals = true;
+    if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite observable or norm on the device");
+    if (status & 1) return fail(c, MSGPU_ERR_EXPM, "run: small matrix exponential failed");
+    return MSGPU_OK;
+}
+
+int msgpu_fetch_yields(msgpu_ctx *c, double *per_traj, double *ensemble)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!c->have_integrals) return fail(c, MSGPU_ERR_STATE, "no yields: run first");
+    if (int rc = device_guard(c)) return rc;
+    const int nobs = static_cast<int>(c->obs.size()), ldm = c->ldm, M = c->M;
+    std::vector<double> acc(static_cast<size_t>(nobs) * ldm);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(acc.data(), c->acc.p, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "fetch yields");
+    for (int o = 0; o < nobs; ++o) {
+        double s = 0.0;
+        for (int t = 0; t < M; ++t) {
+            const double v = acc[static_cast<size_t>(o) * ldm + t];
+            if (per_traj) per_traj[static_cast<size_t>(t) * nobs + o] = v;
+            s += v;
+        }
+        if (ensemble) ensemble[o] = s;
+    }
+    return MSGPU_OK;
+}
+
+int msgpu_fetch_values(msgpu_ctx *c, double *values)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!c->have_integrals || !values) return fail(c, MSGPU_ERR_STATE, "no values: run first");
+    std::copy(c->last_values.begin(), c->last_values.end(), values);
+    return MSGPU_OK;
+}
+
+int msgpu_profile_enable(msgpu_ctx *c, int enable)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    c->prof = enable != 0;
+    for (int k = 0; k < KC_N; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
+    return MSGPU_OK;
+}
+
+int msgpu_profile_read(msgpu_ctx *c, int cls, double *total_ms, long long *launches)
+{
+    if (!c || cls < 0 || cls >= KC_N) return MSGPU_ERR_INVALID;
+    collect_profile(c);
+    if (total_ms) *total_ms = c->prof_ms[cls];
+    if (launches) *launches = c->prof_n[cls];
+    return MSGPU_OK;
+}
+
+}  // extern "C"
+

@@ -1,0 +1,580 @@
+// msgpu_kernels.cuh -- kernels of the streamed Krylov propagation.
+//
+// One propagation step of a block of trajectories is a fixed sequence of
+// kernels on one stream (captured into a CUDA graph by the host):
+//
+//   for j in 0..m-1:    apply   : W = A V_j          (CSR SpMM over the block)
+//                       reduce  : per-trajectory dot products / norms
+//                       orth    : Gram-Schmidt / three-term update
+//   expm                : per-trajectory exp(dt H_m) e1 (one warp each)
+//   combine             : psi = sum_j c_j V_j, singlet-triplet flips,
+//                         electron-pair observables (quartet threads)
+//   yield               : trapezoid accumulation per trajectory
+//
+// Reductions over the Hilbert dimension are two-phase and deterministic:
+// every CTA writes one partial per trajectory, and a separate kernel sums the
+// partials of all row tiles in a fixed order, so a trajectory's result does
+// not depend on how many other trajectories share the launch.
+#pragma once
+
+#include "msgpu_device.cuh"
+
+namespace msgpu {
+
+constexpr int kWarps = 8;            // warps per CTA in the row-tiled kernels
+constexpr int kThreads = 32 * kWarps;
+constexpr int kMaxKrylov = 32;
+
+struct CsrD {
+    const int *rowptr;
+    const int *col;
+    const double2 *val;
+};
+struct CsrF {
+    const int *rowptr;
+    const int *col;
+    const float2 *hi;
+    const float2 *lo;  // may be null: single-word values
+};
+
+// ===================================================================== c128
+// Arnoldi on G = -iH - K with classical Gram-Schmidt applied twice (CGS2),
+// trajectory tile of 32 (one trajectory per lane, 16-byte loads).
+
+// W = G * v_j where v_j = src * scale[t]; also stores v_j into Vj and writes
+// the first-pass partial dots <V_i, W>, i <= j, to part[tile][i][t].
+__global__ void __launch_bounds__(kThreads)
+k_arnoldi_apply(CsrD H, CsrD K, double kappa, const double2 *__restrict__ src, const double *__restrict__ scale,
+                double2 *__restrict__ Vj, double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride,
+                int j, double2 *__restrict__ part, int D, int ldm, int R)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 32 + lane;
+    const int r0 = blockIdx.x * R;
+    const double sc = scale[t];
+    double2 dacc[kMaxKrylov];
+    for (int i = 0; i <= j; ++i) dacc[i] = make_double2(0.0, 0.0);
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        double2 acc = make_double2(0.0, 0.0);
+        const int kb = __ldg(H.rowptr + r), ke = __ldg(H.rowptr + r + 1);
+        for (int k = kb; k < ke; ++k) {
+            const int c = __ldg(H.col + k);
+            const double2 h = __ldg(H.val + k);
+            acc = cfma(h, src[static_cast<size_t>(c) * ldm + t], acc);
+        }
+        acc = cscale(acc, sc);
+        const double2 vr = cscale(src[static_cast<size_t>(r) * ldm + t], sc);
+        double2 g = make_double2(acc.y, -acc.x);  // -i * acc
+        if (K.rowptr) {
+            double2 ka = make_double2(0.0, 0.0);
+            const int qb = __ldg(K.rowptr + r), qe = __ldg(K.rowptr + r + 1);
+            for (int k = qb; k < qe; ++k)
+                ka = cfma(__ldg(K.val + k), src[static_cast<size_t>(__ldg(K.col + k)) * ldm + t], ka);
+            g = csub(g, cscale(ka, sc));
+        } else {
+            g = csub(g, cscale(vr, kappa));
+        }
+        const size_t e = static_cast<size_t>(r) * ldm + t;
+        Vj[e] = vr;
+        W[e] = g;
+        for (int i = 0; i < j; ++i) dacc[i] = cadd(dacc[i], cconjmul(V[i * vstride + e], g));
+        dacc[j] = cadd(dacc[j], cconjmul(vr, g));
+    }
+    __shared__ double2 sm[kWarps][32];
+    for (int i = 0; i <= j; ++i) {
+        sm[warp][lane] = dacc[i];
+        __syncthreads();
+        if (warp == 0) {
+            double2 s = sm[0][lane];
+            for (int w = 1; w < kWarps; ++w) s = cadd(s, sm[w][lane]);
+            part[(static_cast<size_t>(blockIdx.x) * (j + 1) + i) * ldm + t] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// W -= sum_{i<=j} h[i][t] V_i ; then partial dots <V_i, W> (mode 1) or the
+// partial squared norm |W|^2 (mode 2, stored in .x).
+__global__ void __launch_bounds__(kThreads)
+k_arnoldi_orth(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride, int j,
+               const double2 *__restrict__ h, double2 *__restrict__ part, int mode, int D, int ldm, int R)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 32 + lane;
+    const int r0 = blockIdx.x * R;
+    double2 hc[kMaxKrylov];
+    for (int i = 0; i <= j; ++i) hc[i] = h[static_cast<size_t>(i) * ldm + t];
+    double2 dacc[kMaxKrylov];
+    const int nd = mode == 1 ? j + 1 : 1;
+    for (int i = 0; i < nd; ++i) dacc[i] = make_double2(0.0, 0.0);
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        const size_t e = static_cast<size_t>(r) * ldm + t;
+        double2 w = W[e];
+        double2 vi[kMaxKrylov];
+        for (int i = 0; i <= j; ++i) {
+            vi[i] = V[i * vstride + e];
+            w = csub(w, cmul(hc[i], vi[i]));
+        }
+        W[e] = w;
+        if (mode == 1) {
+            for (int i = 0; i <= j; ++i) dacc[i] = cadd(dacc[i], cconjmul(vi[i], w));
+        } else {
+            dacc[0].x += cabs2(w);
+        }
+    }
+    __shared__ double2 sm[kWarps][32];
+    for (int i = 0; i < nd; ++i) {
+        sm[warp][lane] = dacc[i];
+        __syncthreads();
+        if (warp == 0) {
+            double2 s = sm[0][lane];
+            for (int w = 1; w < kWarps; ++w) s = cadd(s, sm[w][lane]);
+            part[(static_cast<size_t>(blockIdx.x) * nd + i) * ldm + t] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// out[i][t] = sum over tiles of part[tile][i][t] (fixed order).
+__global__ void k_reduce_partials(const double2 *__restrict__ part, int ntiles, int ni, int ldm,
+                                  double2 *__restrict__ out)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= ni * ldm) return;
+    const int i = idx / ldm, t = idx % ldm;
+    double2 s = make_double2(0.0, 0.0);
+    for (int tile = 0; tile < ntiles; ++tile) s = cadd(s, part[(static_cast<size_t>(tile) * ni + i) * ldm + t]);
+    out[static_cast<size_t>(i) * ldm + t] = s;
+}
+
+// Per-trajectory Arnoldi bookkeeping after CGS2 of iteration j:
+// H_m[i][j] = h1[i] + h2[i]; beta = |W|; H_m[j+1][j] = beta; scale = 1/beta;
+// a trajectory whose beta falls below 1e-14 (breakdown, as the reference) or
+// that reached the last iteration keeps dimension j+1.
+__global__ void k_arnoldi_finalize(const double2 *__restrict__ h1, const double2 *__restrict__ h2,
+                                   const double2 *__restrict__ nrm, int j, int m, int ldm,
+                                   double2 *__restrict__ hess, int *__restrict__ mdim, double *__restrict__ scale)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ldm) return;
+    const bool active = mdim[t] == 0;
+    double2 *Ht = hess + static_cast<size_t>(t) * m * m;  // column-major m x m
+    for (int i = 0; i <= j; ++i) {
+        const double2 v = cadd(h1[static_cast<size_t>(i) * ldm + t], h2[static_cast<size_t>(i) * ldm + t]);
+        if (active) Ht[i + j * m] = v;
+    }
+    const double beta = sqrt(nrm[t].x);
+    if (!active) { scale[t] = 0.0; return; }
+    if (j == m - 1) { mdim[t] = m; scale[t] = 0.0; return; }
+    Ht[(j + 1) + j * m] = make_double2(beta, 0.0);
+    if (beta < 1e-14) { mdim[t] = j + 1; scale[t] = 0.0; return; }
+    scale[t] = 1.0 / beta;
+}
+
+// ===================================================================== c64
+// Lanczos on H (Hermitian) with complex64 vectors, complex64 H (optionally a
+// hi+lo split), FP64 dot products / norms.  Trajectory tile of 64: each lane
+// carries two trajectories in one 16-byte load.  Vectors are stored
+// unnormalised (w_j) with a per-trajectory scale s_j = 1/|w_j|.
+
+// U = H v_j (v_j = w_j * s_j), partial alpha_j = Re <v_j, U> (FP64).
+template <bool kSplit>
+__global__ void __launch_bounds__(kThreads)
+k_lanczos_apply(CsrF H, const float2 *__restrict__ wj, const double *__restrict__ sj, float2 *__restrict__ U,
+                double *__restrict__ part, int D, int ldm, int R)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 64 + 2 * lane;
+    const int r0 = blockIdx.x * R;
+    const float s0 = static_cast<float>(sj[t]), s1 = static_cast<float>(sj[t + 1]);
+    double a0 = 0.0, a1 = 0.0;
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        float2 acc0 = make_float2(0.f, 0.f), acc1 = make_float2(0.f, 0.f);
+        float2 cor0 = make_float2(0.f, 0.f), cor1 = make_float2(0.f, 0.f);
+        const int kb = __ldg(H.rowptr + r), ke = __ldg(H.rowptr + r + 1);
+        for (int k = kb; k < ke; ++k) {
+            const int c = __ldg(H.col + k);
+            const float2 h = __ldg(H.hi + k);
+            const float4 x = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>(c) * ldm + t);
+            acc0 = cfmaf(h, make_float2(x.x, x.y), acc0);
+            acc1 = cfmaf(h, make_float2(x.z, x.w), acc1);
+            if (kSplit) {
+                const float2 hl = __ldg(H.lo + k);
+                cor0 = cfmaf(hl, make_float2(x.x, x.y), cor0);
+                cor1 = cfmaf(hl, make_float2(x.z, x.w), cor1);
+            }
+        }
+        if (kSplit) {
+            acc0.x += cor0.x; acc0.y += cor0.y;
+            acc1.x += cor1.x; acc1.y += cor1.y;
+        }
+        acc0.x *= s0; acc0.y *= s0; acc1.x *= s1; acc1.y *= s1;
+        const size_t e = static_cast<size_t>(r) * ldm + t;
+        const float4 v = *reinterpret_cast<const float4 *>(wj + e);
+        *reinterpret_cast<float4 *>(U + e) = make_float4(acc0.x, acc0.y, acc1.x, acc1.y);
+        a0 += (static_cast<double>(v.x) * acc0.x + static_cast<double>(v.y) * acc0.y) * s0;
+        a1 += (static_cast<double>(v.z) * acc1.x + static_cast<double>(v.w) * acc1.y) * s1;
+    }
+    __shared__ double sm[kWarps][64];
+    sm[warp][2 * lane] = a0;
+    sm[warp][2 * lane + 1] = a1;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; ++w) s += sm[w][threadIdx.x];
+        part[static_cast<size_t>(blockIdx.x) * ldm + blockIdx.y * 64 + threadIdx.x] = s;
+    }
+}
+
+// w_{j+1} = U - alpha_j v_j - beta_j v_{j-1}; partial |w_{j+1}|^2 (FP64).
+__global__ void __launch_bounds__(kThreads)
+k_lanczos_update(const float2 *__restrict__ U, const float2 *__restrict__ wj, const float2 *__restrict__ wjm1,
+                 const double *__restrict__ sj, const double *__restrict__ sjm1, const double *__restrict__ alpha,
+                 float2 *__restrict__ wn, double *__restrict__ part, int D, int ldm, int R)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 64 + 2 * lane;
+    const int r0 = blockIdx.x * R;
+    // coefficients: alpha*s_j and beta_j*s_{j-1} where beta_j = 1/s_j
+    const float ca0 = static_cast<float>(alpha[t] * sj[t]), ca1 = static_cast<float>(alpha[t + 1] * sj[t + 1]);
+    float cb0 = 0.f, cb1 = 0.f;
+    if (wjm1) {
+        cb0 = sj[t] > 0.0 ? static_cast<float>(sjm1[t] / sj[t]) : 0.f;
+        cb1 = sj[t + 1] > 0.0 ? static_cast<float>(sjm1[t + 1] / sj[t + 1]) : 0.f;
+    }
+    double n0 = 0.0, n1 = 0.0;
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        const size_t e = static_cast<size_t>(r) * ldm + t;
+        const float4 u = *reinterpret_cast<const float4 *>(U + e);
+        const float4 v = *reinterpret_cast<const float4 *>(wj + e);
+        float4 o;
+        o.x = fmaf(-ca0, v.x, u.x); o.y = fmaf(-ca0, v.y, u.y);
+        o.z = fmaf(-ca1, v.z, u.z); o.w = fmaf(-ca1, v.w, u.w);
+        if (wjm1) {
+            const float4 p = *reinterpret_cast<const float4 *>(wjm1 + e);
+            o.x = fmaf(-cb0, p.x, o.x); o.y = fmaf(-cb0, p.y, o.y);
+            o.z = fmaf(-cb1, p.z, o.z); o.w = fmaf(-cb1, p.w, o.w);
+        }
+        *reinterpret_cast<float4 *>(wn + e) = o;
+        n0 += static_cast<double>(o.x) * o.x + static_cast<double>(o.y) * o.y;
+        n1 += static_cast<double>(o.z) * o.z + static_cast<double>(o.w) * o.w;
+    }
+    __shared__ double sm[kWarps][64];
+    sm[warp][2 * lane] = n0;
+    sm[warp][2 * lane + 1] = n1;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; ++w) s += sm[w][threadIdx.x];
+        part[static_cast<size_t>(blockIdx.x) * ldm + blockIdx.y * 64 + threadIdx.x] = s;
+    }
+}
+
+// out[t] = sum over tiles of part[tile][t] (fixed order), optional sqrt and
+// Lanczos bookkeeping: mode 0 -> alpha_j (stored to T diag), mode 1 -> beta_{j+1}
+// (stored to T offdiag, scale = 1/beta, breakdown marks the dimension).
+__global__ void k_lanczos_reduce(const double *__restrict__ part, int ntiles, int ldm, int mode, int j, int m,
+                                 double *__restrict__ out, double *__restrict__ tdiag, double *__restrict__ toff,
+                                 int *__restrict__ mdim)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ldm) return;
+    double s = 0.0;
+    for (int tile = 0; tile < ntiles; ++tile) s += part[static_cast<size_t>(tile) * ldm + t];
+    const bool active = mdim[t] == 0;
+    if (mode == 0) {
+        out[t] = s;
+        if (active) {
+            tdiag[static_cast<size_t>(t) * m + j] = s;
+            if (j == m - 1) mdim[t] = m;
+        }
+        return;
+    }
+    const double beta = sqrt(s);
+    if (!active) { out[t] = 0.0; return; }
+    if (j == m - 1) { mdim[t] = m; out[t] = 0.0; return; }
+    toff[static_cast<size_t>(t) * m + j] = beta;
+    if (beta < 1e-14) { mdim[t] = j + 1; out[t] = 0.0; return; }
+    out[t] = 1.0 / beta;
+}
+
+// ===================================================================== shared
+// Per-trajectory small exponential: y = beta0 * exp(dt*A_m) e1 where A_m is
+// the Arnoldi Hessenberg matrix of G (hess != null) or -iT - kappa I from the
+// Lanczos tridiagonal (tdiag/toff).  One warp per trajectory.  coef[t][j]
+// receives y_j times the storage scale of basis vector j (vscale, may be null).
+__global__ void k_krylov_expm(const double2 *__restrict__ hess, const double *__restrict__ tdiag,
+                              const double *__restrict__ toff, double kappa, const int *__restrict__ mdim,
+                              const double *__restrict__ beta0, const double *__restrict__ vscale, int m,
+                              int ldm, int M, double dt, double2 *__restrict__ coef, int *__restrict__ status)
+{
+    extern __shared__ double2 smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (t >= ldm) return;
+    double2 *A = smem + static_cast<size_t>(warp) * (4 * m * m + m);
+    double2 *X = A + m * m, *N = X + m * m, *Dm = N + m * m, *y = Dm + m * m;
+    const int n = max(1, mdim[t]);
+    const double b0 = beta0[t];
+    if (lane < n) {
+        for (int i = 0; i < n; ++i) {
+            double2 v;
+            if (hess) {
+                v = hess[static_cast<size_t>(t) * m * m + i + lane * m];
+            } else {
+                v = make_double2(0.0, 0.0);
+                if (i == lane) v = make_double2(-kappa, -tdiag[static_cast<size_t>(t) * m + i]);
+                else if (i == lane + 1) v = make_double2(0.0, -toff[static_cast<size_t>(t) * m + lane]);
+                else if (i + 1 == lane) v = make_double2(0.0, -toff[static_cast<size_t>(t) * m + i]);
+            }
+            A[i + lane * n] = cscale(v, dt);
+        }
+    }
+    __syncwarp();
+    bool ok = true;
+    if (b0 > 0.0) ok = warp_expm_col0(n, A, X, N, Dm, y);
+    if (lane < m) {
+        double2 c = make_double2(0.0, 0.0);
+        if (b0 > 0.0 && ok && lane < n) {
+            c = cscale(y[lane], b0);
+            if (vscale) c = cscale(c, vscale[static_cast<size_t>(lane) * ldm + t]);
+        }
+        coef[static_cast<size_t>(t) * m + lane] = c;
+    }
+    if (!ok && lane == 0 && t < M) atomicOr(status, 1);
+}
+
+// Flip bit for trajectory t at (global step, half): replay bits (layout
+// ((step*2+half)*M + t)) or Philox.
+struct Noise {
+    int mode;                // 0 none, 1 replay bits, 2 philox
+    const uint8_t *bits;     // replay
+    long long bits_steps;    // number of steps covered by bits
+    int M;                   // trajectories in the bit layout
+    uint64_t seed;           // philox
+    uint32_t traj_offset;    // philox trajectory id offset
+    double p_full;           // flip probability for a half step of the current step
+};
+
+__device__ __forceinline__ int noise_bit(const Noise &nz, int t, long long step, int half, double p)
+{
+    if (step < 0) return 0;
+    if (nz.mode == 1) {
+        if (t >= nz.M || step < 0 || step >= nz.bits_steps) return 0;
+        const long long bit = (step * 2 + half) * nz.M + t;
+        return (nz.bits[bit >> 3] >> (bit & 7)) & 1;
+    }
+    if (nz.mode == 2)
+        return philox_flip(nz.seed, nz.traj_offset + static_cast<uint32_t>(t), static_cast<uint32_t>(step),
+                           static_cast<uint32_t>(half), p) ? 1 : 0;
+    return 0;
+}
+
+struct PairObs {
+    int nobs;
+    double2 op[8][16];  // 4x4 row-major in the pair basis
+};
+
+// Quartet epilogue shared by both precisions: apply the singlet-triplet flip
+// U = PS - PT (x4 -> -(swap middle), negate ends) when flip is set, and add
+// <x|O_o|x> to obs[o] and |x|^2 to nrm.
+__device__ __forceinline__ void quartet_epilogue(double2 x[4], int flip, const PairObs &po, double *obs, double &nrm)
+{
+    if (flip) {
+        const double2 a = x[1];
+        x[0] = make_double2(-x[0].x, -x[0].y);
+        x[1] = make_double2(-x[2].x, -x[2].y);
+        x[2] = make_double2(-a.x, -a.y);
+        x[3] = make_double2(-x[3].x, -x[3].y);
+    }
+    nrm += cabs2(x[0]) + cabs2(x[1]) + cabs2(x[2]) + cabs2(x[3]);
+    for (int o = 0; o < po.nobs; ++o) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double2 ox = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) ox = cfma(po.op[o][a * 4 + b], x[b], ox);
+            s += x[a].x * ox.x + x[a].y * ox.y;  // Re(conj(x_a) (O x)_a)
+        }
+        obs[o] += s;
+    }
+}
+
+// psi = sum_{j<n_t} coef[t][j] V_j at the four rows of each quartet, then the
+// combined flip of this half step pair, observables and norm partials.
+// kBasis=false evaluates psi itself (start of a run: flip of the first half
+// step only, no Krylov combination).
+template <typename T, bool kBasis>
+__global__ void __launch_bounds__(256)
+k_combine(T *__restrict__ psi, const T *__restrict__ V, size_t vstride, const double2 *__restrict__ coef,
+          const int *__restrict__ mdim, int m, int s1, int s2, int Q, int ldm, int QR, Noise nz, long long stepA,
+          int halfA, double pA, long long stepB, int halfB, double pB, PairObs po, double *__restrict__ part_obs,
+          double *__restrict__ part_nrm)
+{
+    // blockDim = (32, 8): x over trajectories, y over quartets of the tile
+    const int t = blockIdx.y * 32 + threadIdx.x;
+    const int q0 = blockIdx.x * QR;
+    double obs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double nrm = 0.0;
+    const int n = kBasis ? max(1, mdim[t]) : 0;
+    int flip = noise_bit(nz, t, stepA, halfA, pA);
+    if (stepB >= 0) flip ^= noise_bit(nz, t, stepB, halfB, pB);
+    for (int q = q0 + threadIdx.y; q < min(q0 + QR, Q); q += blockDim.y) {
+        const int base = quartet_base(q, s1, s2);
+        size_t e[4];
+        e[0] = static_cast<size_t>(base) * ldm + t;
+        e[1] = static_cast<size_t>(base + s2) * ldm + t;
+        e[2] = static_cast<size_t>(base + s1) * ldm + t;
+        e[3] = static_cast<size_t>(base + s1 + s2) * ldm + t;
+        double2 x[4];
+        if (kBasis) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) x[a] = make_double2(0.0, 0.0);
+            for (int jj = 0; jj < n; ++jj) {
+                const double2 c = coef[static_cast<size_t>(t) * m + jj];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const T v = V[jj * vstride + e[a]];
+                    x[a] = cfma(c, make_double2(v.x, v.y), x[a]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) { const T v = psi[e[a]]; x[a] = make_double2(v.x, v.y); }
+        }
+        quartet_epilogue(x, flip, po, obs, nrm);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            T o;
+            o.x = x[a].x;
+            o.y = x[a].y;
+            psi[e[a]] = o;
+        }
+    }
+    __shared__ double sm[9][8][33];
+    for (int o = 0; o < po.nobs; ++o) sm[o][threadIdx.y][threadIdx.x] = obs[o];
+    sm[8][threadIdx.y][threadIdx.x] = nrm;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        for (int o = 0; o < po.nobs; ++o) {
+            double s = 0.0;
+            for (int w = 0; w < blockDim.y; ++w) s += sm[o][w][threadIdx.x];
+            part_obs[(static_cast<size_t>(blockIdx.x) * po.nobs + o) * ldm + t] = s;
+        }
+        double s = 0.0;
+        for (int w = 0; w < blockDim.y; ++w) s += sm[8][w][threadIdx.x];
+        part_nrm[static_cast<size_t>(blockIdx.x) * ldm + t] = s;
+    }
+}
+
+// Per-trajectory trapezoid accumulation (compensated) of the observable
+// values of this time point; init=1 only records the first value.
+// Also refreshes beta0 = |psi| and the inverse scale of the next step, and
+// optionally writes the ensemble value (sum over trajectories < M) of this
+// time point to values_out[o].  Launch with one CTA of 1024 threads.
+__global__ void k_yield_update(const double *__restrict__ part_obs, const double *__restrict__ part_nrm,
+                               int ntiles, int nobs, int ldm, int M, const double *__restrict__ rates, double dt,
+                               int init, double *__restrict__ prev, double *__restrict__ acc,
+                               double *__restrict__ comp, double *__restrict__ beta0, double *__restrict__ inv0,
+                               double *__restrict__ values_out, int *__restrict__ status)
+{
+    __shared__ double red[8][32];
+    double ens[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool bad = false;
+    for (int t = threadIdx.x; t < ldm; t += blockDim.x) {
+        for (int o = 0; o < nobs; ++o) {
+            double v = 0.0;
+            for (int tile = 0; tile < ntiles; ++tile) v += part_obs[(static_cast<size_t>(tile) * nobs + o) * ldm + t];
+            v *= rates[o];
+            const size_t k = static_cast<size_t>(o) * ldm + t;
+            if (!init) {
+                // Kahan-compensated acc += 0.5*dt*(prev+v)
+                const double term = 0.5 * dt * (prev[k] + v) - comp[k];
+                const double s = acc[k] + term;
+                comp[k] = (s - acc[k]) - term;
+                acc[k] = s;
+            }
+            prev[k] = v;
+            if (t < M) ens[o] += v;
+            if (!isfinite(v)) bad = true;
+        }
+        double nn = 0.0;
+        for (int tile = 0; tile < ntiles; ++tile) nn += part_nrm[static_cast<size_t>(tile) * ldm + t];
+        const double b = sqrt(nn);
+        beta0[t] = b;
+        inv0[t] = b > 0.0 ? 1.0 / b : 0.0;
+        if (!isfinite(b)) bad = true;
+    }
+    if (bad) atomicOr(status, 2);
+    if (!values_out) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 0; o < nobs; ++o) {
+        double v = warp_sum(ens[o]);
+        if (lane == 0) red[o][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nobs) {
+        double s = 0.0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        values_out[threadIdx.x] = s;
+    }
+}
+
+template <typename Dst, typename Src>
+__global__ void k_convert(Dst *__restrict__ out, const Src *__restrict__ in, size_t n)
+{
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Dst o;
+    o.x = in[i].x;
+    o.y = in[i].y;
+    out[i] = o;
+}
+
+
+// Column-major D x M (one trajectory per column, as HSPreparedState factors)
+// <-> trajectory-interleaved (row r, trajectory t at r*ldm + t), through 32x32
+// shared-memory tiles so both sides stay coalesced.  Padding trajectories
+// M <= t < ldm are written as zero.
+template <typename Dst>
+__global__ void k_cols_to_interleaved(Dst *__restrict__ out, const double2 *__restrict__ in, int D, int M, int ldm)
+{
+    __shared__ double2 tile[32][33];
+    const int r0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int t = t0 + k, r = r0 + threadIdx.x;
+        tile[k][threadIdx.x] = (t < M && r < D) ? in[static_cast<size_t>(t) * D + r] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, t = t0 + threadIdx.x;
+        if (r < D && t < ldm) {
+            Dst o;
+            o.x = tile[threadIdx.x][k].x;
+            o.y = tile[threadIdx.x][k].y;
+            out[static_cast<size_t>(r) * ldm + t] = o;
+        }
+    }
+}
+
+template <typename Src>
+__global__ void k_interleaved_to_cols(double2 *__restrict__ out, const Src *__restrict__ in, int D, int M, int ldm)
+{
+    __shared__ double2 tile[32][33];
+    const int r0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, t = t0 + threadIdx.x;
+        if (r < D && t < ldm) {
+            const Src v = in[static_cast<size_t>(r) * ldm + t];
+            tile[k][threadIdx.x] = make_double2(v.x, v.y);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int t = t0 + k, r = r0 + threadIdx.x;
+        if (t < M && r < D) out[static_cast<size_t>(t) * D + r] = tile[threadIdx.x][k];
+    }
+}
+
+}  // namespace msgpu

@@ -1,0 +1,40 @@
+"""The C ABI library loads and exports every symbol its headers declare."""
+import os
+import re
+import subprocess
+
+from molspin_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for hdr in ("msgpu.h", "msgpu_host.h"):
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(msgpu_\w+)\s*\(", text))
+    return names
+
+
+def test_all_declared_symbols_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (msgpu_\w+)", out))
+    declared = _declared()
+    assert declared, "no declarations parsed"
+    missing = declared - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+    for name in declared:
+        assert hasattr(L.lib, name)
+
+
+def test_library_targets_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", L.LIB_PATH], capture_output=True, text=True)
+    if out.returncode == 0:
+        assert "sm_100a" in out.stdout
+
+
+def test_null_context_errors():
+    assert L.lib.msgpu_last_error(None) == b"null context"
+    assert L.lib.msgpu_run(None, None) == L.MSGPU_ERR_INVALID
+    assert L.lib.msgpu_upload_hamiltonian_csr(None, 4, None, None, None) == L.MSGPU_ERR_INVALID

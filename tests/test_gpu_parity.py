@@ -1,0 +1,209 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances (written per test): per-trajectory yields of the complex128 form
+within 1e-10 relative of the oracle; exact-trace ensembles within 1e-10 of
+the density oracle; stochastic ensembles within the reference's 6 sigma bound
+6/(2 sqrt(M)); Haberkorn survival within 2e-6 (reference bound).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from molspin_b200 import _lib as L
+from molspin_b200 import hsgeneral as hs
+from molspin_b200 import systems as S
+from oracle import density as den
+from oracle import pyoracle as orc
+from tests import helpers as h
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(system, factors, times, krylov, precision="c128", noise=None, K_csr=None, kappa=None,
+         obs=None, chunks=None):
+    with hs.HSPropagatorB200(0) as p:
+        p.set_hamiltonian(*system.hamiltonian_csr())
+        if K_csr is not None:
+            p.set_reaction(csr=K_csr)
+        else:
+            p.set_reaction(kappa=system.kappa() if kappa is None else kappa)
+        p.set_electron_pair(*system.electron_strides())
+        obs = obs if obs is not None else [(op, rate) for _, op, rate in system.observables()]
+        p.set_observables(obs)
+        if noise is not None:
+            p.set_noise(*noise)
+        p.set_factors(factors)
+        if chunks is None:
+            p.propagate(times, krylov, precision)
+            values = p.values()
+        else:
+            values = []
+            start = 0
+            for k, stop in enumerate(chunks):
+                p.propagate(times[start:stop + 1], krylov, precision, step_offset=start, accumulate=k > 0)
+                values.append(p.values() if k == 0 else p.values()[1:])
+                start = stop
+            values = np.concatenate(values)
+        per, ens = p.yields()
+        return per, ens, values, p.get_factors()
+
+
+def _oracle(system, factors, times, krylov, U=False, **kw):
+    obs = h.oracle_observables(system)
+    if U:
+        kw["U_csr"] = orc.st_unitary(system.mult, *system.electrons)
+        kw["event_rate"] = 0.5 * system.st_rate
+    return orc.hs_stochastic(system.hamiltonian_csr(), factors, times, obs, krylov=krylov, nthreads=8, **kw)
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+def test_plain_per_trajectory_parity_config1_shape():
+    w = S.plain_small()
+    M, steps = 64, 200
+    times = S.time_grid(steps * w.dt, w.dt)
+    F = w.system.trace_samples(M, w.seed)
+    per, ens, values, Fg = _gpu(w.system, F, times, w.krylov)
+    ref = _oracle(w.system, F, times, w.krylov, kappa=w.system.kappa())
+    assert _rel(per, ref["traj_yield"]) < 1e-10
+    assert _rel(ens, ref["yield"]) < 1e-10
+    assert _rel(values, ref["values"]) < 1e-10
+    assert np.max(np.abs(Fg - ref["factors"])) < 1e-10 * np.max(np.abs(ref["factors"]))
+
+
+def test_plain_parity_reference_noise_stream():
+    system = h.random_system([2, 2, 2], [2], seed=11, st_rate=0.05, sink=2e-3, hf_scale=3.0)
+    M, times = 100, S.time_grid(60.0, 0.5)
+    F = system.trace_samples(M, 7.0)
+    bits = hs.reference_flip_bits(7.0, system.st_rate, times, M, orientation=0)
+    assert np.unpackbits(bits).sum() > 50
+    per, ens, _, _ = _gpu(system, F, times, 12, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
+    ref = _oracle(system, F, times, 12, U=True, kappa=system.kappa(), noise_mode=0, seed=7.0, seed_mode=0)
+    assert _rel(per, ref["traj_yield"]) < 1e-10
+    assert _rel(ens, ref["yield"]) < 1e-10
+
+
+def test_plain_parity_philox_replayed_on_cpu():
+    system = h.random_system([2, 3], [2, 2], seed=12, st_rate=0.08, hf_scale=3.0)
+    M, times = 70, S.time_grid(40.0, 1.0)
+    F = system.trace_samples(M, 3.0)
+    seed = 0xDEADBEEF1234
+    per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_PHILOX, seed))
+    bits = hs.philox_flip_bits(seed, system.st_rate, times, M)
+    ref = _oracle(system, F, times, 16, U=True, kappa=system.kappa(), noise_mode=1, flip_bits=bits)
+    assert _rel(per, ref["traj_yield"]) < 1e-10
+
+
+def test_plain_parity_general_K_and_interleaved_electrons():
+    # electrons at positions 1 and 3 (neither leading), unequal sinks -> CSR K
+    s = S.SpinSystem(mult=[2, 2, 3, 2, 2], names=["N1", "E1", "N2", "E2", "N3"], electrons=(1, 3))
+    rng = np.random.default_rng(4)
+    for e in (1, 3):
+        s.linear.append((e, S.COMMON_PREFACTOR * 2.0023 * 1e-4 * rng.normal(size=3)))
+    for e, n in ((1, 0), (1, 2), (3, 4)):
+        s.bilinear.append((e, n, S.COMMON_PREFACTOR * 2.0023e-3 * S._aniso_tensor(rng, 2.0)))
+    s.sinks = {"S": 3e-3, "T0": 1e-3, "Tp": 1e-3, "Tm": 1e-3}
+    s.st_rate = 0.0
+    K = sum(0.5 * rate * den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), s) for n, rate in s.sinks.items())
+    Kc = den.to_csr(K, 1e-18)
+    M = 45
+    F = rng.normal(size=(s.dim, M)) + 1j * rng.normal(size=(s.dim, M))
+    F /= np.linalg.norm(F, axis=0) * math.sqrt(M)
+    times = S.time_grid(30.0, 1.0)
+    obs = [(op, rate) for _, op, rate in s.observables()]
+    per, ens, _, _ = _gpu(s, F, times, 10, K_csr=Kc, obs=obs)
+    ref = orc.hs_stochastic(s.hamiltonian_csr(), F, times, h.oracle_observables(s), K_csr=Kc, krylov=10)
+    assert _rel(per, ref["traj_yield"]) < 1e-10
+
+
+def test_exact_trace_against_density_oracle():
+    system = h.random_system([2, 2], [2], seed=21, hf_scale=2.0)
+    times = S.time_grid(80.0, 1.0)
+    F = den.orthonormal_nuclear_samples(system, S.SINGLET)
+    _, ens, values, _ = _gpu(system, F, times, 16)
+    H = den.dense_hamiltonian(system)
+    K = system.kappa() * np.eye(system.dim)
+    ops = [(den.pair_operator(op, system), rate) for _, op, rate in system.observables()]
+    dv, dy = den.propagate_density(H, K, den.singlet_density(system), times, ops)
+    assert _rel(ens, dy) < 1e-10
+    assert _rel(values, dv) < 1e-10
+
+
+def test_stochastic_st_against_lindblad_and_survival():
+    # GeneralStatic fixture of the reference on the GPU (8192 samples, m=8)
+    system = h.st_fixture()
+    times = S.time_grid(2.0, 0.025)
+    M = 8192
+    F = system.trace_samples(M, 431.0)
+    pops = [(S.pair_projector(S.PAIR_STATES[n]), 1.0) for n in ("S", "T0", "Tp", "Tm")]
+    bits = hs.reference_flip_bits(431.0, 0.7, times, M)
+    _, _, values, _ = _gpu(system, F, times, 8, noise=(0.7, L.NOISE_REPLAY, 0, bits, len(times) - 1, M), obs=pops)
+    assert np.max(np.abs(values.sum(axis=1) - np.exp(-0.2 * times))) < 2e-6
+    H = den.dense_hamiltonian(system)
+    K = 0.1 * np.eye(system.dim)
+    rho0 = den.singlet_density(system)
+    U = den.st_unitary(system)
+    direct = np.array([[np.trace(den.pair_operator(op, system) @ den.lindblad_exact(H, K, rho0, t, U, 0.7)).real
+                        for op, _ in pops] for t in times])
+    assert np.max(np.abs(values - direct)) < h.six_sigma(M)
+
+
+def test_chunked_run_is_bitwise_identical():
+    system = h.random_system([2, 2, 2], [2, 2], seed=31, st_rate=0.05, hf_scale=2.0)
+    M, times = 64, S.time_grid(40.0, 1.0)
+    F = system.trace_samples(M, 5.0)
+    noise = (system.st_rate, L.NOISE_PHILOX, 99)
+    a = _gpu(system, F, times, 12, noise=noise)
+    b = _gpu(system, F, times, 12, noise=noise, chunks=[13, 27, 40])
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[2], b[2])
+
+
+def test_precision_form_against_plain():
+    w = S.precision_large(M=64, steps=40)
+    F = w.system.trace_samples(64, 1.0)
+    times = S.time_grid(40 * w.dt, w.dt)
+    per64, ens64, val64, _ = _gpu(w.system, F, times, w.krylov, precision="c64")
+    per128, ens128, val128, _ = _gpu(w.system, F, times, w.krylov, precision="c128")
+    # singlet yield (observable 0): ensemble within 1e-6 relative of the complex128 path
+    assert abs(ens64[0] - ens128[0]) <= 1e-6 * abs(ens128[0])
+    assert np.max(np.abs(val64 - val128)) <= 1e-6 * np.max(np.abs(val128))
+
+
+def test_full_size_survival_property():
+    # size-independent law at the benchmark size D=16384: with K = k/2 I the
+    # population summed over S, T0, T+, T- decays exactly as exp(-k t)
+    w = S.precision_large(M=64, steps=6)
+    F = w.system.trace_samples(64, 1.0)
+    times = S.time_grid(6 * w.dt, w.dt)
+    k = 1e-3
+    pops = [(S.pair_projector(S.PAIR_STATES[n]), 1.0) for n in ("S", "T0", "Tp", "Tm")]
+    for prec, tol in (("c128", 1e-12), ("c64", 2e-6)):
+        _, _, values, _ = _gpu(w.system, F, times, w.krylov, precision=prec, obs=pops)
+        assert np.max(np.abs(values.sum(axis=1) - np.exp(-k * times))) < tol
+
+
+def test_error_paths():
+    system = h.random_system([2, 2], [2], seed=3)
+    r, c, v = system.hamiltonian_csr()
+    with hs.HSPropagatorB200(0) as p:
+        bad = v.copy()
+        bad[0] = np.nan
+        with pytest.raises(hs.MsgpuError) as e:
+            p.set_hamiltonian(r, c, bad)
+        assert e.value.code == L.MSGPU_ERR_NONFINITE
+        with pytest.raises(hs.MsgpuError) as e:
+            p.propagate(S.time_grid(2.0, 1.0), 8)
+        assert e.value.code == L.MSGPU_ERR_STATE
+        p.set_hamiltonian(r, c, v)
+        with pytest.raises(hs.MsgpuError) as e:
+            p.set_electron_pair(4, 4)
+        assert e.value.code == L.MSGPU_ERR_INVALID
+    with hs.HSPropagatorB200(0, hbm_budget=4096) as p:
+        with pytest.raises(hs.MsgpuError) as e:
+            p.set_hamiltonian(r, c, v)
+            p.set_factors(system.trace_samples(64, 1.0))
+        assert e.value.code == L.MSGPU_ERR_BUDGET

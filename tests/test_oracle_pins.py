@@ -1,0 +1,243 @@
+"""Pins of the CPU oracle against the reference's own known-answer tests.
+
+The reference cannot be built here (no Armadillo), so each test below restates
+one of its stochastic-path tests with the same inputs, seeds and bounds and
+runs it on the oracle (oracle/hs_oracle.cpp) or the density oracle
+(oracle/density.py).  Reference file: Tests/tests_StochasticRelaxation.cpp
+unless noted.
+"""
+import math
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from molspin_b200 import systems as S
+from oracle import density as den
+from oracle import pyoracle as orc
+from tests import helpers as h
+
+
+def _pair_density_inputs(system):
+    H = den.dense_hamiltonian(system)
+    K = 0.5 * system.sinks["S"] * np.eye(system.dim)
+    return H, K
+
+
+def test_time_grid_exact_endpoint():
+    # TaskHSGeneral.cpp:59-96: integer-indexed targets, exact final point
+    t = orc.time_grid(2.0, 0.025)
+    assert len(t) == 81 and t[-1] == 2.0 and t[40] == 40 * 0.025
+    t = orc.time_grid(0.1, 0.03)
+    assert np.allclose(t, [0, 0.03, 0.06, 0.09, 0.1]) and t[-1] == 0.1
+    assert list(orc.time_grid(0.0, 1.0)) == [0.0]
+    np.testing.assert_array_equal(S.time_grid(0.1, 0.03), t)
+
+
+def test_expm_against_scipy():
+    rng = np.random.default_rng(5)
+    for n, scale in [(1, 1.0), (4, 0.3), (16, 5.0), (20, 40.0)]:
+        A = scale * (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))) / math.sqrt(n)
+        E = orc.expm(A)
+        R = sla.expm(A)
+        assert np.linalg.norm(E - R) <= 1e-12 * max(1.0, np.linalg.norm(R))
+
+
+def test_krylov_full_dimension_is_exact():
+    system = h.random_system([2, 2, 3], [2], seed=7)
+    Hc = system.hamiltonian_csr()
+    H = den.dense_hamiltonian(system)
+    rng = np.random.default_rng(1)
+    b = rng.normal(size=system.dim) + 1j * rng.normal(size=system.dim)
+    kappa, dt = 0.05, 3.0
+    exact = sla.expm(dt * (-1j * H - kappa * np.eye(system.dim))) @ b
+    got = orc.krylov_expm(Hc, kappa, b, dt, system.dim)
+    assert np.linalg.norm(got - exact) <= 1e-11 * np.linalg.norm(exact)
+    got16 = orc.krylov_expm(Hc, kappa, b, dt, 16)
+    assert np.linalg.norm(got16 - exact) <= 1e-8 * np.linalg.norm(exact)
+
+
+def test_st_algebra():
+    # Algebra (:49-72): PS, PT projectors; U = PS - PT unitary and involutory
+    r, c, v = orc.st_unitary([2, 2], 0, 1)
+    U = np.zeros((4, 4), complex)
+    for i in range(4):
+        U[i, c[r[i]:r[i + 1]]] = v[r[i]:r[i + 1]]
+    I = np.eye(4)
+    assert np.linalg.norm(U @ U - I) < 1e-13 and np.linalg.norm(U.conj().T @ U - I) < 1e-13
+    PS = 0.5 * (U + I)
+    assert np.linalg.norm(PS @ PS - PS) < 1e-13
+    assert np.linalg.norm(PS - S.pair_projector(S.SINGLET)) < 1e-13
+    # the density oracle's U is the same matrix
+    assert np.linalg.norm(den.st_unitary(h.st_fixture(nucleus=False)) - U) < 1e-13
+
+
+def test_st_analytic_law_and_norm():
+    # AnalyticAndNorm (:73-93)
+    Uc = orc.st_unitary([2, 2], 0, 1)
+    N, t, k = 32768, 1.3, 0.7
+    F = np.zeros((4, N), complex)
+    F[1, :] = 0.6
+    F = orc.apply_st(Uc, 0.5 * k, t, 519, F)
+    rho = F @ F.conj().T / N
+    p = -math.expm1(-k * t) / 2.0
+    sigma = 0.36 * math.sqrt(p * (1 - p) / N)
+    assert abs(rho[2, 2].real - 0.36 * p) <= 6 * sigma
+    assert abs(np.trace(rho).real - 0.36) <= 1e-12
+    assert np.all(np.abs((np.abs(F) ** 2).sum(axis=0) - 0.36) <= 1e-13)
+    s = np.array([0, 1, -1, 0]) / math.sqrt(2)
+    tr = np.array([0, 1, 1, 0]) / math.sqrt(2)
+    assert abs((s.conj() @ rho @ tr).real - 0.18 * math.exp(-k * t)) < 6 * sigma
+    assert abs((s.conj() @ rho @ s).real - 0.18) < 1e-12
+    assert abs((tr.conj() @ rho @ tr).real - 0.18) < 1e-12
+
+
+def test_st_monte_carlo_rms():
+    # MonteCarloConvergence (:398-418)
+    Uc = orc.st_unitary([2, 2], 0, 1)
+    p = -0.5 * math.expm1(-0.7)
+    rms = []
+    for n in (256, 1024, 4096):
+        mse = 0.0
+        for seed in range(1, 65):
+            B = np.zeros((4, n), complex)
+            B[1, :] = 1.0
+            B = orc.apply_st(Uc, 0.35, 1.0, seed, B)
+            est = (np.abs(B[2, :]) ** 2).sum() / n
+            mse += (est - p) ** 2
+        rms.append(math.sqrt(mse / 64))
+        expected = math.sqrt(p * (1 - p) / n)
+        assert 0.5 * expected <= rms[-1] <= 1.5 * expected
+    assert rms[0] / rms[-1] > 2.5
+
+
+def test_st_reproducibility_and_noop():
+    # ReproducibilityAndNoop (:114-130) at the full-loop level: a zero-rate
+    # Operator is a no-op and consumes no random numbers; equal seeds repeat.
+    system = h.st_fixture()
+    times = orc.time_grid(0.2, 0.05)
+    F = orc.trace_samples(71, S.SINGLET, 2, 32)
+    Hc = h.dense_csr(system)
+    obs = h.state_population_observables(system)
+    Uc = orc.st_unitary(system.mult, 0, 1)
+    base = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8)
+    zero = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.0, seed=71)
+    np.testing.assert_array_equal(base["values"], zero["values"])
+    a = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.35, seed=71)
+    b = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.35, seed=71)
+    np.testing.assert_array_equal(a["values"], b["values"])
+    assert not np.array_equal(a["factors"], base["factors"])
+    assert not orc.st_flip_bits(71, 0, 0, 0.0, times, 32).any()
+    # explicit bits of the same stream replay the same trajectories exactly
+    bits = orc.st_flip_bits(71, 0, 0, 0.35, times, 32)
+    c = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.35, noise_mode=1,
+                          flip_bits=bits)
+    np.testing.assert_array_equal(a["values"], c["values"])
+
+
+@pytest.mark.slow
+def test_general_static_survival_and_density():
+    # GeneralStatic (:197-217): E1,E2,N; 4 sinks k=0.2; Z = 0.8 Sz(E1); ST 0.7;
+    # totaltime 2, timestep 0.025, seed 431, 8192 samples, krylov m=8.
+    system = h.st_fixture()
+    times = orc.time_grid(2.0, 0.025)
+    M = 8192
+    F = orc.trace_samples(431, S.SINGLET, 2, M)
+    Hc = h.dense_csr(system)
+    obs = h.state_population_observables(system)
+    Uc = orc.st_unitary(system.mult, 0, 1)
+    out = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.35, seed=431,
+                            nthreads=8)
+    surv = out["values"].sum(axis=1)
+    assert np.max(np.abs(surv - np.exp(-0.2 * times))) < 2e-6
+    H, K = _pair_density_inputs(system)
+    rho0 = den.singlet_density(system)
+    ops = [(den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), system), 1.0) for n in ("S", "T0", "Tp", "Tm")]
+    # the reference's "direct" arm: exact Lindblad dynamics at every grid point
+    direct = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t, den.st_unitary(system), 0.7)).real
+                        for O, _ in ops] for t in times])
+    err = np.max(np.abs(out["values"] - direct))
+    assert err < h.six_sigma(M), err
+    # the coherent (no-ST) direct answer is far away, so the check has teeth
+    coherent = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t)).real for O, _ in ops] for t in times])
+    assert abs(direct[-1, 0] - coherent[-1, 0]) > 0.07
+
+
+def test_split_second_order():
+    # SplitConvergence (:371-397) on the density oracle's split map
+    system = h.st_fixture(nucleus=False)
+    H = 1.9 * den.embed({0: den.spin_matrices(2)[2]}, [2, 2])
+    K = np.zeros((4, 4))
+    U = den.st_unitary(system)
+    psi = S.SINGLET
+    rho0 = np.outer(psi, psi.conj())
+    exact = den.lindblad_exact(H, K, rho0, 1.0, U, 0.7)
+    errs = []
+    for steps in (5, 10, 20, 40):
+        times = np.arange(steps + 1) / steps
+        _, _, rho = den.propagate_density(H, K, rho0, times, [], U, 0.7, return_rho=True)
+        errs.append(np.linalg.norm(rho - exact))
+    for a, b in zip(errs, errs[1:]):
+        assert 3.8 <= a / b <= 4.2
+
+
+def test_noncommuting_trajectory_convergence():
+    # NoncommutingMonteCarloConvergence (:466-499): exponential propagator,
+    # H = 1.9 Sz(E1), K = 0, dt = 0.05, 20 steps, std::mt19937(seed) directly.
+    system = h.st_fixture(nucleus=False)
+    H = 1.9 * den.embed({0: den.spin_matrices(2)[2]}, [2, 2])
+    Hc = den.to_csr(H)
+    U = den.st_unitary(system)
+    Uc = den.to_csr(U, 1e-15)
+    psi = S.SINGLET
+    times = np.arange(21) * 0.05
+    _, _, rho = den.propagate_density(H, np.zeros((4, 4)), np.outer(psi, psi.conj()), times, [], U, 0.7,
+                                      return_rho=True)
+    expected = (psi.conj() @ rho @ psi).real
+    P = den.to_csr(np.outer(psi, psi.conj()))
+    errors = []
+    for n in (256, 1024, 4096):
+        mse = 0.0
+        for seed in range(1, 33):
+            B = np.repeat(psi[:, None], n, axis=1)
+            out = orc.hs_stochastic(Hc, B, times, [(P, 1.0)], method=1, U_csr=Uc, event_rate=0.35, seed=seed,
+                                    seed_mode=1)
+            est = out["values"][-1, 0] / n
+            mse += (est - expected) ** 2
+        errors.append(math.sqrt(mse / 32))
+        assert errors[-1] <= 3 / math.sqrt(n)
+    assert errors[0] / errors[-1] > 2.5
+
+
+def test_yield_correction_closed_form():
+    # test_hsgeneral_yield_correction_matches_finite_decay_law
+    # (Tests/tests_HSGeneral.cpp:1085-1112): one sink on S with rate 0.02,
+    # totaltime 0.5, timestep 0.05, yieldcorrections=true.
+    rate, total, dt = 0.02, 0.5, 0.05
+    system = h.st_fixture(field=False, nucleus=False, st_rate=0.0)
+    times = orc.time_grid(total, dt)
+    PS = den.pair_operator(S.pair_projector(S.SINGLET), system)
+    Kc = den.to_csr(0.5 * rate * PS)
+    Hc = (np.arange(5, dtype=np.int32) * 0, np.zeros(0, np.int32), np.zeros(0, complex))
+    out = orc.hs_stochastic(Hc, S.SINGLET[:, None], times, [(den.to_csr(PS), rate)], K_csr=Kc, krylov=4)
+    trapezoid = sum(0.5 * dt * rate * (math.exp(-rate * (s - 1) * dt) + math.exp(-rate * s * dt))
+                    for s in range(1, 11))
+    expected = trapezoid / (1.0 - math.exp(-rate * total))
+    got = out["yield"][0] * orc.yield_correction(total, rate)
+    assert abs(got - expected) < 1e-10
+
+
+def test_trace_sampling_structure():
+    # test_hsgeneral_stochastic_preparation_remains_factorized (tests_HSGeneral.cpp:1155-1188):
+    # E1, E2 + spin-1 N, singlet fixed, 5 samples -> 12 x 5 factors, Z = 3
+    F = orc.trace_samples(17, S.SINGLET, 3, 5)
+    assert F.shape == (12, 5)
+    assert np.allclose(np.linalg.norm(F, axis=0), 1 / math.sqrt(5), atol=1e-15)
+    P = np.kron(S.pair_projector(S.SINGLET), np.eye(3))
+    assert np.linalg.norm(P @ F - F) < 1e-14
+    # SU(Z) density oracle (tests_StochasticRelaxation.cpp:518-582 style)
+    M = 8192
+    F = orc.trace_samples(71, S.SINGLET, 2, M)
+    rho = F @ F.conj().T
+    target = np.kron(S.pair_projector(S.SINGLET), np.eye(2) / 2)
+    assert np.linalg.norm(rho - target) < 6 / math.sqrt(M)
