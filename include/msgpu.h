@@ -137,6 +137,35 @@ int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long 
 /* Number of kernels this context launched since creation. */
 long long msgpu_launch_count(const msgpu_ctx *ctx);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (for example code running inside a CUDA-graph capture or under a
+ * memory pool that forbids cudaMalloc, or a host framework that owns all
+ * allocations): one Krylov step psi_out = exp(dt (-iH - kappa I)) psi_in for
+ * every trajectory column, computed with the complex128 Arnoldi kernels of
+ * msgpu_run, using only the caller's buffers and a fixed static scratch area
+ * of MSGPU_NOALLOC_SCRATCH_BYTES compiled into this library (held on every
+ * GPU that loads it, until the process exits).  It calls no cudaMalloc or
+ * cudaFree.
+ *   - rowptr/col/val (CSR of H in rad/ns, val interleaved complex128),
+ *     psi_in and psi_out (dim x ntraj column-major complex128) are DEVICE
+ *     pointers; psi_in and psi_out must not overlap.  dim must be a multiple
+ *     of 4 (a radical pair is always present).
+ *   - Problems whose working set does not fit the scratch area are rejected
+ *     with MSGPU_ERR_SCRATCH before any work is queued; with krylov_dim 16 the
+ *     area holds, e.g., dim 64 with up to 512 trajectories.
+ *   - The first call on a device looks up the scratch address on that device
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one scratch area: calls that may overlap on the GPU
+ *     (different streams, or several host threads) race and must be
+ *     serialised by the caller.
+ * Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream)
+ * and the call waits for it to finish. */
+#define MSGPU_ERR_SCRATCH 8
+#define MSGPU_NOALLOC_SCRATCH_BYTES (16u << 20)
+int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *col, const double *val, double kappa,
+                              int ntraj, const double *psi_in, double *psi_out, double dt, int krylov_dim,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,8 @@ MSGPU_ERR_NONFINITE = 3
 MSGPU_ERR_EXPM = 4
 MSGPU_ERR_CUDA = 6
 MSGPU_ERR_STATE = 7
+MSGPU_ERR_SCRATCH = 8
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 PREC_C128 = 0
 PREC_C64 = 1
@@ -81,6 +83,7 @@ def _load() -> C.CDLL:
         "msgpu_profile_enable": (I, [P, I]),
         "msgpu_profile_read": (I, [P, I, pD, C.POINTER(C.c_longlong)]),
         "msgpu_launch_count": (C.c_longlong, [P]),
+        "msgpu_krylov_step_noalloc": (I, [I, P, P, P, D, I, P, P, D, I, P]),
         "msgpu_host_build_hamiltonian": (C.c_longlong, [I, pI, I, pI, pD, I, pI, pI, pD, pI, pI, pD]),
         "msgpu_host_trace_samples": (I, [D, pD, I, I, I, pD]),
         "msgpu_host_reference_flip_bits": (I, [D, I, C.c_ulonglong, D, pD, I, I, pU8]),

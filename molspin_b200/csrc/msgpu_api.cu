@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -837,4 +838,173 @@ int msgpu_profile_read(msgpu_ctx *c, int cls, double *total_ms, long long *launc
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Allocation-free Krylov step (msgpu_krylov_step_noalloc).
+//
+// Some callers cannot call cudaMalloc: code that runs while a stream is being
+// captured into a CUDA graph, hosts whose memory pool owns every device
+// allocation, or embedders that must bound device memory at load time.  For
+// them this entry point runs one complex128 Arnoldi step with all of its
+// temporaries in one static device array.  The array lives in this library
+// image, so every GPU that loads the library holds MSGPU_NOALLOC_SCRATCH_BYTES
+// until the process exits.  Host code may not use the array's name as a
+// device address (on the host it names a stand-in object), so the address is
+// looked up once per device with cudaGetSymbolAddress and passed to kernels.
+// ============================================================================
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MSGPU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up on
+// the first call per device).
+cudaError_t noalloc_scratch(void **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+// Carves 256-byte aligned sub-buffers out of the scratch array.
+struct Carve {
+    unsigned char *base;
+    size_t off = 0;
+    template <typename T>
+    T *take(size_t n)
+    {
+        T *p = reinterpret_cast<T *>(base + off);
+        off += (n * sizeof(T) + 255) / 256 * 256;
+        return p;
+    }
+};
+
+}  // namespace
+
+extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *col, const double *val,
+                                         double kappa, int ntraj, const double *psi_in, double *psi_out, double dt,
+                                         int krylov_dim, void *stream)
+{
+    if (dim < 4 || dim % 4 != 0 || ntraj <= 0 || !rowptr || !col || !val || !psi_in || !psi_out)
+        return MSGPU_ERR_INVALID;
+    if (krylov_dim < 1 || krylov_dim > kMaxKrylov || !std::isfinite(dt) || !(dt > 0.0) || !std::isfinite(kappa))
+        return MSGPU_ERR_INVALID;
+    const int D = dim, m = std::min(krylov_dim, dim);
+    const int ldm = (ntraj + 63) / 64 * 64;
+    const size_t n = static_cast<size_t>(D) * ldm;
+    const int R = pick_rows_per_tile(D), nt = ceil_div(D, R);
+    const int Q = D / 4, QR = std::max(8, std::min(256, Q / 64)), qt = ceil_div(Q, QR);
+    // Sizes of every temporary, checked against the static capacity before
+    // anything is queued.
+    Carve probe{nullptr};
+    probe.take<double2>(n);                                  // interleaved state
+    probe.take<double2>(n * m);                              // Krylov basis
+    probe.take<double2>(n);                                  // W
+    probe.take<double2>(n);                                  // Z
+    probe.take<double2>(static_cast<size_t>(nt) * (m + 1) * ldm);  // partials
+    probe.take<double2>(static_cast<size_t>(3) * (m + 1) * ldm);   // dots
+    probe.take<double2>(static_cast<size_t>(ldm) * m * m);   // Hessenberg
+    probe.take<double2>(static_cast<size_t>(ldm) * m);       // coefficients
+    probe.take<int>(ldm);                                    // Krylov dims
+    probe.take<double>(static_cast<size_t>(m + 1) * ldm);    // scales
+    probe.take<double>(ldm);                                 // beta0
+    probe.take<double>(static_cast<size_t>(qt) * ldm);       // norm partials
+    probe.take<double>(8);                                   // observable partials (none used)
+    probe.take<int>(1);                                      // status
+    if (probe.off > MSGPU_NOALLOC_SCRATCH_BYTES) return MSGPU_ERR_SCRATCH;
+
+    void *base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess) return MSGPU_ERR_CUDA;
+    Carve cv{static_cast<unsigned char *>(base)};
+    double2 *psi = cv.take<double2>(n);
+    double2 *V = cv.take<double2>(n * m);
+    double2 *bufA = cv.take<double2>(n);
+    double2 *bufB = cv.take<double2>(n);
+    double2 *part = cv.take<double2>(static_cast<size_t>(nt) * (m + 1) * ldm);
+    double2 *dots = cv.take<double2>(static_cast<size_t>(3) * (m + 1) * ldm);
+    double2 *hess = cv.take<double2>(static_cast<size_t>(ldm) * m * m);
+    double2 *coef = cv.take<double2>(static_cast<size_t>(ldm) * m);
+    int *mdim = cv.take<int>(ldm);
+    double *sc = cv.take<double>(static_cast<size_t>(m + 1) * ldm);
+    double *beta0 = cv.take<double>(ldm);
+    double *qnrm = cv.take<double>(static_cast<size_t>(qt) * ldm);
+    double *qobs = cv.take<double>(8);
+    int *status = cv.take<int>(1);
+
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    // Contents left by the previous call are stale: clear what must start at zero.
+    if ((e = cudaMemsetAsync(status, 0, sizeof(int), st)) || (e = cudaMemsetAsync(mdim, 0, ldm * sizeof(int), st)))
+        return MSGPU_ERR_CUDA;
+    {
+        dim3 grid(ceil_div(D, 32), ldm / 32), block(32, 8);
+        k_cols_to_interleaved<double2><<<grid, block, 0, st>>>(psi, reinterpret_cast<const double2 *>(psi_in), D,
+                                                               ntraj, ldm);
+    }
+    PairObs po;
+    std::memset(&po, 0, sizeof(po));
+    Noise nz;
+    std::memset(&nz, 0, sizeof(nz));
+    dim3 qgrid(qt, ldm / 32), qblock(32, 8);
+    // any two spin-1/2 digit strides partition the rows into quartets; without
+    // observables or flips only the norms are read from the quartet pass
+    const int s1 = D / 2, s2 = D / 4;
+    k_combine<double2, false><<<qgrid, qblock, 0, st>>>(psi, nullptr, 0, nullptr, nullptr, m, s1, s2, Q, ldm, QR, nz,
+                                                        -1, 0, 0.0, -1, 0, 0.0, po, qobs, qnrm);
+    k_yield_update<<<1, 1024, 0, st>>>(qobs, qnrm, qt, 0, ldm, ntraj, nullptr, 0.0, 1, nullptr, nullptr, nullptr,
+                                       beta0, sc, nullptr, status);
+    CsrD Hd{rowptr, col, reinterpret_cast<const double2 *>(val)};
+    CsrD Kd{nullptr, nullptr, nullptr};
+    double2 *h1 = dots, *h2 = dots + static_cast<size_t>(m + 1) * ldm, *nr = dots + 2 * static_cast<size_t>(m + 1) * ldm;
+    const double2 *src = psi;
+    double2 *W = bufA;
+    dim3 grid(nt, ldm / 32);
+    for (int j = 0; j < m; ++j) {
+        k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, V, n, j,
+                                                   part, D, ldm, R);
+        k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(part, nt, j + 1, ldm, h1);
+        k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h1, part, 1, D, ldm, R);
+        k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(part, nt, j + 1, ldm, h2);
+        k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h2, part, 2, D, ldm, R);
+        k_reduce_partials<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, 1, ldm, nr);
+        k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(h1, h2, nr, j, m, ldm, hess, mdim, sc + ldm);
+        src = W;
+        W = (W == bufA) ? bufB : bufA;
+    }
+    const size_t smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
+    const int warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / smem_warp)));
+    if ((e = cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(warps * smem_warp))))
+        return MSGPU_ERR_CUDA;
+    k_krylov_expm<<<ceil_div(ldm, warps), 32 * warps, warps * smem_warp, st>>>(hess, nullptr, nullptr, 0.0, mdim, beta0,
+                                                                              nullptr, m, ldm, ntraj, dt, coef, status);
+    k_combine<double2, true><<<qgrid, qblock, 0, st>>>(psi, V, n, coef, mdim, m, s1, s2, Q, ldm, QR, nz, -1, 0, 0.0,
+                                                       -1, 0, 0.0, po, qobs, qnrm);
+    {
+        dim3 g(ceil_div(D, 32), ldm / 32), b(32, 8);
+        k_interleaved_to_cols<double2><<<g, b, 0, st>>>(reinterpret_cast<double2 *>(psi_out), psi, D, ntraj, ldm);
+    }
+    if ((e = cudaGetLastError())) return MSGPU_ERR_CUDA;
+    int h_status = 0;
+    if ((e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+        return MSGPU_ERR_CUDA;
+    if (h_status & 2) return MSGPU_ERR_NONFINITE;
+    if (h_status & 1) return MSGPU_ERR_EXPM;
+    return MSGPU_OK;
+}
 
