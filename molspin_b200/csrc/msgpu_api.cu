@@ -38,6 +38,13 @@ struct msgpu_ctx {
     // Hamiltonian
     int D = 0, nnz = 0;
     DevBuf hrow, hcol, hval, hhi, hlo;
+    std::vector<int> h_rowptr, h_col;  // host copy for the quartet-block form
+    std::vector<double> h_val;
+    // quartet-block form of H for the current electron strides
+    DevBuf qrow, qcolt, qval, qbase;
+    int q_s1 = 0, q_s2 = 0, q_D = 0, q_nblocks = 0;
+    int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
+    int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
     // reaction
     bool k_scalar = true;
     double kappa = 0.0;
@@ -212,7 +219,8 @@ void msgpu_destroy(msgpu_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     collect_profile(c);
-    DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->krow, &c->kcol, &c->kval, &c->bits,
+    DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->qrow, &c->qcolt, &c->qval, &c->qbase,
+                     &c->krow, &c->kcol, &c->kval, &c->bits,
                      &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d};
@@ -277,6 +285,10 @@ int msgpu_upload_hamiltonian_csr(msgpu_ctx *c, int dim, const int *rowptr, const
     if ((e = cudaStreamSynchronize(c->stream))) return cuda_fail(c, e, "Hamiltonian upload");
     c->D = dim;
     c->nnz = nnz;
+    c->h_rowptr.assign(rowptr, rowptr + dim + 1);
+    c->h_col.assign(col, col + nnz);
+    c->h_val.assign(val, val + 2 * static_cast<size_t>(nnz));
+    c->q_D = 0;  // quartet form must be rebuilt
     return MSGPU_OK;
 }
 
@@ -452,7 +464,8 @@ int ensure_workspace(msgpu_ctx *c, int prec, int m)
         // w_0 (= state) .. w_m, and U
         if ((rc = ensure(c, c->basis, n * (m + 1) * sizeof(float2), "Lanczos basis")) ||
             (rc = ensure(c, c->ubuf, n * sizeof(float2), "Lanczos U")) ||
-            (rc = ensure(c, c->part, static_cast<size_t>(c->ntiles) * ldm * sizeof(double), "partials")) ||
+            (rc = ensure(c, c->part, static_cast<size_t>(std::max(c->ntiles, ceil_div(Q, 8))) * ldm * sizeof(double),
+                         "partials")) ||
             (rc = ensure(c, c->tdiag, static_cast<size_t>(ldm) * m * sizeof(double), "T diagonal")) ||
             (rc = ensure(c, c->toff, static_cast<size_t>(ldm) * m * sizeof(double), "T offdiagonal")) ||
             (rc = ensure(c, c->alpha, static_cast<size_t>(ldm) * sizeof(double), "alpha")))
@@ -480,19 +493,19 @@ int ensure_workspace(msgpu_ctx *c, int prec, int m)
 int ensure_state(msgpu_ctx *c, int prec)
 {
     if (c->state_prec == prec) return MSGPU_OK;
-    const size_t n = static_cast<size_t>(c->D) * c->ldm;
+    const size_t npairs = static_cast<size_t>(c->D) * c->ldm / 2;
     const int threads = 256;
-    const int blocks = ceil_div(static_cast<long long>(n), threads);
+    const int blocks = ceil_div(static_cast<long long>(npairs), threads);
     if (prec == MSGPU_PREC_C64 && c->state_prec == MSGPU_PREC_C128) {
         Timed tm(c, KC_COMBINE);
-        k_convert<float2, double2><<<blocks, threads, 0, c->stream>>>(static_cast<float2 *>(c->basis.p),
-                                                                      static_cast<const double2 *>(c->psi128.p), n);
+        k_c128_to_pp<<<blocks, threads, 0, c->stream>>>(static_cast<float4 *>(c->basis.p),
+                                                         static_cast<const double2 *>(c->psi128.p), npairs);
     } else if (prec == MSGPU_PREC_C128 && c->state_prec == MSGPU_PREC_C64) {
-        // the c64 basis may have been released by a workspace switch; keep it
-        // alive by converting before any reallocation (see msgpu_run)
+        // msgpu_run parks the complex64 state here before the basis buffer is
+        // reused or reallocated
         Timed tm(c, KC_COMBINE);
-        k_convert<double2, float2><<<blocks, threads, 0, c->stream>>>(static_cast<double2 *>(c->psi128.p),
-                                                                      static_cast<const float2 *>(c->basis.p), n);
+        k_pp_to_c128<<<blocks, threads, 0, c->stream>>>(static_cast<double2 *>(c->psi128.p),
+                                                         static_cast<const float4 *>(c->basis.p), npairs);
     } else {
         return fail(c, MSGPU_ERR_STATE, "no trajectory state uploaded");
     }
@@ -503,6 +516,164 @@ int ensure_state(msgpu_ctx *c, int prec)
 }
 
 double flip_p(double st_rate, double h) { return -0.5 * std::expm1(-2.0 * (0.5 * st_rate) * h); }
+
+// Quartet-block form of H for the current electron strides (see QuartetC).
+int build_quartet(msgpu_ctx *c)
+{
+    if (c->q_D == c->D && c->q_s1 == c->s1 && c->q_s2 == c->s2) return MSGPU_OK;
+    const int D = c->D, s1 = c->s1, s2 = c->s2, Q = D / 4;
+    const int off[4] = {0, s2, s1, s1 + s2};
+    std::vector<int> rowptr(Q + 1, 0), base(Q);
+    std::vector<int2> blks;
+    std::vector<float> vals;
+    std::vector<std::pair<int, std::array<double, 32>>> blocks;  // (neighbour base, 16 complex)
+    for (int q = 0; q < Q; ++q) {
+        const int lo = q % s2, mid = (q / s2) % (s1 / (2 * s2)), hi = q / (s1 / 2);
+        const int b = hi * (2 * s1) + mid * (2 * s2) + lo;
+        base[q] = b;
+        blocks.clear();
+        for (int a = 0; a < 4; ++a) {
+            const int r = b + off[a];
+            for (int k = c->h_rowptr[r]; k < c->h_rowptr[r + 1]; ++k) {
+                const int col = c->h_col[k];
+                const int a1 = (col / s1) & 1, a2 = (col / s2) & 1;
+                const int cb = col - a1 * s1 - a2 * s2, bi = 2 * a1 + a2;
+                size_t slot = 0;
+                while (slot < blocks.size() && blocks[slot].first != cb) ++slot;
+                if (slot == blocks.size()) {
+                    std::array<double, 32> z;
+                    z.fill(0.0);
+                    blocks.push_back({cb, z});
+                }
+                blocks[slot].second[2 * (a * 4 + bi)] += c->h_val[2 * static_cast<size_t>(k)];
+                blocks[slot].second[2 * (a * 4 + bi) + 1] += c->h_val[2 * static_cast<size_t>(k) + 1];
+            }
+        }
+        std::sort(blocks.begin(), blocks.end(), [](auto &x, auto &y) { return x.first < y.first; });
+        for (auto &blk : blocks) {
+            const auto &B = blk.second;  // 16 complex, row-major in the pair index
+            auto re = [&](int a, int b) { return B[2 * (a * 4 + b)]; };
+            auto im = [&](int a, int b) { return B[2 * (a * 4 + b) + 1]; };
+            double bmax = 0.0;
+            bool e1only = true, e2only = true;
+            for (int a = 0; a < 4; ++a)
+                for (int bb = 0; bb < 4; ++bb) {
+                    bmax = std::max(bmax, std::abs(re(a, bb)) + std::abs(im(a, bb)));
+                    const bool nz = re(a, bb) != 0.0 || im(a, bb) != 0.0;
+                    if (!nz) continue;
+                    if ((a & 1) != (bb & 1)) e1only = false;  // couples different second digits
+                    if ((a & 2) != (bb & 2)) e2only = false;  // couples different first digits
+                }
+            auto same = [&](int a, int b, int a2, int b2) {
+                return std::abs(re(a, b) - re(a2, b2)) + std::abs(im(a, b) - im(a2, b2)) <= 1e-13 * bmax;
+            };
+            // emit (a, b) pairs of the block in the storage order of its type
+            std::vector<std::pair<int, int>> order;
+            int type;
+            if (e1only && e2only) {
+                type = 3;
+                for (int a = 0; a < 4; ++a) order.push_back({a, a});
+            } else if (e1only) {
+                // acts on the first digit; A (x) I when both second-digit halves agree
+                const bool kron = same(0, 0, 1, 1) && same(0, 2, 1, 3) && same(2, 0, 3, 1) && same(2, 2, 3, 3);
+                type = kron ? 4 : 1;
+                for (int a2 = 0; a2 < (kron ? 1 : 2); ++a2)
+                    for (int a1 = 0; a1 < 2; ++a1)
+                        for (int b1 = 0; b1 < 2; ++b1) order.push_back({2 * a1 + a2, 2 * b1 + a2});
+            } else if (e2only) {
+                const bool kron = same(0, 0, 2, 2) && same(0, 1, 2, 3) && same(1, 0, 3, 2) && same(1, 1, 3, 3);
+                type = kron ? 5 : 2;
+                for (int a1 = 0; a1 < (kron ? 1 : 2); ++a1)
+                    for (int a2 = 0; a2 < 2; ++a2)
+                        for (int b2 = 0; b2 < 2; ++b2) order.push_back({2 * a1 + a2, 2 * a1 + b2});
+            } else {
+                type = 0;
+                for (int a = 0; a < 4; ++a)
+                    for (int bb = 0; bb < 4; ++bb) order.push_back({a, bb});
+            }
+            blks.push_back({(blk.first << 3) | type, static_cast<int>(vals.size() / 4)});
+            for (auto &ab : order) {
+                vals.push_back(static_cast<float>(re(ab.first, ab.second)));
+                vals.push_back(static_cast<float>(im(ab.first, ab.second)));
+            }
+        }
+        rowptr[q + 1] = static_cast<int>(blks.size());
+    }
+    const int nb = static_cast<int>(blks.size());
+    int rc;
+    if ((rc = ensure(c, c->qrow, sizeof(int) * (Q + 1), "quartet rowptr")) ||
+        (rc = ensure(c, c->qcolt, sizeof(int2) * std::max(1, nb), "quartet blocks")) ||
+        (rc = ensure(c, c->qval, sizeof(float) * std::max<size_t>(4, vals.size()), "quartet values")) ||
+        (rc = ensure(c, c->qbase, sizeof(int) * Q, "quartet bases")))
+        return rc;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->qrow.p, rowptr.data(), sizeof(int) * (Q + 1), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->qcolt.p, blks.data(), sizeof(int2) * nb, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->qval.p, vals.data(), sizeof(float) * vals.size(), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->qbase.p, base.data(), sizeof(int) * Q, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "quartet upload");
+    c->q_D = D;
+    c->q_s1 = s1;
+    c->q_s2 = s2;
+    c->q_nblocks = nb;
+    c->q_tile = 0;
+    return MSGPU_OK;
+}
+
+QuartetC quartet_view(const msgpu_ctx *c)
+{
+    return QuartetC{static_cast<const int *>(c->qrow.p), static_cast<const int2 *>(c->qcolt.p),
+                    static_cast<const float4 *>(c->qval.p), static_cast<const int *>(c->qbase.p)};
+}
+
+// Autotuner for the quartet SpMM: times each candidate tile (quartets per
+// CTA) on the context's own data with CUDA events and keeps the fastest for
+// this (D, trajectory block).  Runs once per context and shape.
+using ApplyFn = void (*)(QuartetC, const float2 *, const double *, float2 *, double *, int, int, int, int, int);
+const ApplyFn kApplyVariants[] = {
+    k_lanczos_apply_compact<true, 2>,
+    k_lanczos_apply_compact<true, 3>,
+    k_lanczos_apply_compact<false, 3>,
+    k_lanczos_apply_compact<false, 4>,
+};
+constexpr int kNumApplyVariants = sizeof(kApplyVariants) / sizeof(kApplyVariants[0]);
+
+int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U, double *part)
+{
+    if (c->q_tile && c->q_tile_ldm == c->ldm) return MSGPU_OK;
+    const int Q = c->D / 4;
+    const int cand[] = {8, 16, 32, 64, 128};
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    int best_qt = 32, best_v = 0;
+    for (int v = 0; v < kNumApplyVariants; ++v)
+        for (int qt : cand) {
+            if (qt > Q && qt != cand[0]) continue;
+            dim3 grid(ceil_div(Q, qt), c->ldm / 64);
+            kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
+                                                                c->ldm, qt);
+            cudaEventRecord(a, c->stream);
+            for (int rep = 0; rep < 3; ++rep)
+                kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
+                                                                    c->ldm, qt);
+            cudaEventRecord(b, c->stream);
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best) { best = ms; best_qt = qt; best_v = v; }
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaError_t e = cudaGetLastError();
+    if (e) return cuda_fail(c, e, "quartet tile tuning");
+    c->q_tile = best_qt;
+    c->q_variant = best_v;
+    c->q_tile_ldm = c->ldm;
+    return MSGPU_OK;
+}
 
 }  // namespace
 
@@ -524,21 +695,15 @@ int msgpu_download_factors(msgpu_ctx *c, double *factors)
     if (c->state_prec < 0 || !factors) return fail(c, MSGPU_ERR_STATE, "no trajectory state to download");
     if (int rc = device_guard(c)) return rc;
     const size_t sbytes = static_cast<size_t>(c->D) * c->M * sizeof(double2);
-    if (c->state_prec == MSGPU_PREC_C128 && c->ws_prec != MSGPU_PREC_C128) {
-        if (int rc = ensure(c, c->zbuf, sbytes, "download staging")) return rc;
-    }
-    if (c->zbuf.bytes < sbytes) {
-        if (int rc = ensure(c, c->zbuf, sbytes, "download staging")) return rc;
-    }
+    // a complex64 state is widened into the complex128 state first (exact)
+    if (c->state_prec == MSGPU_PREC_C64)
+        if (int rc = ensure_state(c, MSGPU_PREC_C128)) return rc;
+    if (int rc = ensure(c, c->zbuf, sbytes, "download staging")) return rc;
     dim3 grid(ceil_div(c->D, 32), c->ldm / 32), block(32, 8);
     {
         Timed tm(c, KC_COMBINE);
-        if (c->state_prec == MSGPU_PREC_C128)
-            k_interleaved_to_cols<double2><<<grid, block, 0, c->stream>>>(
-                static_cast<double2 *>(c->zbuf.p), static_cast<const double2 *>(c->psi128.p), c->D, c->M, c->ldm);
-        else
-            k_interleaved_to_cols<float2><<<grid, block, 0, c->stream>>>(
-                static_cast<double2 *>(c->zbuf.p), static_cast<const float2 *>(c->basis.p), c->D, c->M, c->ldm);
+        k_interleaved_to_cols<double2><<<grid, block, 0, c->stream>>>(
+            static_cast<double2 *>(c->zbuf.p), static_cast<const double2 *>(c->psi128.p), c->D, c->M, c->ldm);
     }
     cudaError_t e;
     if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(factors, c->zbuf.p, sbytes, cudaMemcpyDeviceToHost, c->stream)) ||
@@ -644,19 +809,23 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 steps > 0 ? g0 : -1, 0, pstep(0), sB, 0, 0.0, po, static_cast<double *>(c->qpart_obs.p),
                 static_cast<double *>(c->qpart_nrm.p));
         else
-            k_combine<float2, false><<<qgrid, qblock, 0, st>>>(
-                static_cast<float2 *>(c->basis.p), nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz,
+            k_combine_pp<false><<<dim3(qt, ldm / 64), qblock, 0, st>>>(
+                static_cast<float2 *>(c->basis.p), nullptr, 0, nullptr, nullptr, c->s1, c->s2, Q, ldm, QR, nz,
                 steps > 0 ? g0 : -1, 0, pstep(0), sB, 0, 0.0, po, static_cast<double *>(c->qpart_obs.p),
                 static_cast<double *>(c->qpart_nrm.p));
     }
     yield_update(0.0, 1, 0);
+    if (prec == MSGPU_PREC_C64) {
+        if (int rc = build_quartet(c)) return rc;
+        if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc, static_cast<float2 *>(c->ubuf.p),
+                                       static_cast<double *>(c->part.p)))
+            return rc;
+    }
 
     const int R = c->rows_per_tile, nt = c->ntiles;
     CsrD Hd{static_cast<const int *>(c->hrow.p), static_cast<const int *>(c->hcol.p), static_cast<const double2 *>(c->hval.p)};
     CsrD Kd{c->k_scalar ? nullptr : static_cast<const int *>(c->krow.p), static_cast<const int *>(c->kcol.p),
             static_cast<const double2 *>(c->kval.p)};
-    CsrF Hf{static_cast<const int *>(c->hrow.p), static_cast<const int *>(c->hcol.p), static_cast<const float2 *>(c->hhi.p),
-            nullptr};
     const double kappa = c->k_scalar ? c->kappa : 0.0;
     const size_t expm_smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
     const int expm_warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / expm_smem_warp)));
@@ -684,7 +853,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_REDUCE);
-                    k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(
+                    k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(
                         static_cast<double2 *>(c->part.p), nt, j + 1, ldm, h1);
                 }
                 {
@@ -693,7 +862,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_REDUCE);
-                    k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(
+                    k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(
                         static_cast<double2 *>(c->part.p), nt, j + 1, ldm, h2);
                 }
                 {
@@ -702,7 +871,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_REDUCE);
-                    k_reduce_partials<<<ceil_div(ldm, 256), 256, 0, st>>>(static_cast<double2 *>(c->part.p), nt, 1, ldm, nr);
+                    k_reduce_partials<<<dim3(ldm / 32, 1), dim3(32, 8), 0, st>>>(static_cast<double2 *>(c->part.p), nt, 1, ldm, nr);
                     k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(h1, h2, nr, j, mws, ldm,
                                                                            static_cast<double2 *>(c->hess.p),
                                                                            static_cast<int *>(c->mdim.p), sc + ldm);
@@ -732,15 +901,17 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             double *alpha = static_cast<double *>(c->alpha.p);
             double *td = static_cast<double *>(c->tdiag.p), *to = static_cast<double *>(c->toff.p);
             dim3 grid(nt, ldm / 64);
+            const int QT = c->q_tile, nqt = ceil_div(Q, QT);
+            dim3 qgrid_apply(nqt, ldm / 64);
             for (int j = 0; j < m; ++j) {
                 {
                     Timed tm(c, KC_APPLY);
-                    k_lanczos_apply<false><<<grid, kThreads, 0, st>>>(Hf, Wb + j * n, sc + static_cast<size_t>(j) * ldm, U,
-                                                                     part, D, ldm, R);
+                    kApplyVariants[c->q_variant]<<<qgrid_apply, kThreads, 0, st>>>(
+                        quartet_view(c), Wb + j * n, sc + static_cast<size_t>(j) * ldm, U, part, Q, c->s1, c->s2, ldm, QT);
                 }
                 {
                     Timed tm(c, KC_REDUCE);
-                    k_lanczos_reduce<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, ldm, 0, j, mws, alpha, td, to,
+                    k_lanczos_reduce<<<ldm / 32, dim3(32, 8), 0, st>>>(part, nqt, ldm, 0, j, mws, alpha, td, to,
                                                                          static_cast<int *>(c->mdim.p));
                 }
                 if (j == m - 1) break;  // T_m is complete; w_m is never used
@@ -752,7 +923,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_REDUCE);
-                    k_lanczos_reduce<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, ldm, 1, j, mws,
+                    k_lanczos_reduce<<<ldm / 32, dim3(32, 8), 0, st>>>(part, nt, ldm, 1, j, mws,
                                                                          sc + static_cast<size_t>(j + 1) * ldm, td, to,
                                                                          static_cast<int *>(c->mdim.p));
                 }
@@ -765,9 +936,9 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             }
             {
                 Timed tm(c, KC_COMBINE);
-                k_combine<float2, true><<<qgrid, qblock, 0, st>>>(
-                    Wb, Wb, n, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->mdim.p), mws, c->s1, c->s2, Q,
-                    ldm, QR, nz, g, 1, pstep(s), s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po,
+                k_combine_pp<true><<<dim3(qt, ldm / 64), qblock, 0, st>>>(
+                    Wb, Wb, n, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->mdim.p), c->s1, c->s2, Q, ldm,
+                    QR, nz, g, 1, pstep(s), s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po,
                     static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p));
             }
         }
@@ -976,11 +1147,11 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
     for (int j = 0; j < m; ++j) {
         k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, V, n, j,
                                                    part, D, ldm, R);
-        k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(part, nt, j + 1, ldm, h1);
+        k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(part, nt, j + 1, ldm, h1);
         k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h1, part, 1, D, ldm, R);
-        k_reduce_partials<<<ceil_div(static_cast<long long>(j + 1) * ldm, 256), 256, 0, st>>>(part, nt, j + 1, ldm, h2);
+        k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(part, nt, j + 1, ldm, h2);
         k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h2, part, 2, D, ldm, R);
-        k_reduce_partials<<<ceil_div(ldm, 256), 256, 0, st>>>(part, nt, 1, ldm, nr);
+        k_reduce_partials<<<dim3(ldm / 32, 1), dim3(32, 8), 0, st>>>(part, nt, 1, ldm, nr);
         k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(h1, h2, nr, j, m, ldm, hess, mdim, sc + ldm);
         src = W;
         W = (W == bufA) ? bufB : bufA;

@@ -136,14 +136,21 @@ k_arnoldi_orth(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vs
 }
 
 // out[i][t] = sum over tiles of part[tile][i][t] (fixed order).
+// Launch with blockDim (32, 8) and (ldm/32, ni) blocks; fixed summation order.
 __global__ void k_reduce_partials(const double2 *__restrict__ part, int ntiles, int ni, int ldm,
                                   double2 *__restrict__ out)
 {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= ni * ldm) return;
-    const int i = idx / ldm, t = idx % ldm;
+    __shared__ double2 red[8][33];
+    const int t = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y;
+    double2 ps = make_double2(0.0, 0.0);
+    for (int tile = threadIdx.y; tile < ntiles; tile += 8)
+        ps = cadd(ps, part[(static_cast<size_t>(tile) * ni + i) * ldm + t]);
+    red[threadIdx.y][threadIdx.x] = ps;
+    __syncthreads();
+    if (threadIdx.y != 0) return;
     double2 s = make_double2(0.0, 0.0);
-    for (int tile = 0; tile < ntiles; ++tile) s = cadd(s, part[(static_cast<size_t>(tile) * ni + i) * ldm + t]);
+#pragma unroll
+    for (int y = 0; y < 8; ++y) s = cadd(s, red[y][threadIdx.x]);
     out[static_cast<size_t>(i) * ldm + t] = s;
 }
 
@@ -177,43 +184,179 @@ __global__ void k_arnoldi_finalize(const double2 *__restrict__ h1, const double2
 // carries two trajectories in one 16-byte load.  Vectors are stored
 // unnormalised (w_j) with a per-trajectory scale s_j = 1/|w_j|.
 
-// U = H v_j (v_j = w_j * s_j), partial alpha_j = Re <v_j, U> (FP64).
-template <bool kSplit>
-__global__ void __launch_bounds__(kThreads)
-k_lanczos_apply(CsrF H, const float2 *__restrict__ wj, const double *__restrict__ sj, float2 *__restrict__ U,
-                double *__restrict__ part, int D, int ldm, int R)
+// ---------------------------------------------------------------- quartet SpMM
+// H in quartet-block form: the rows of an electron-pair quartet (the four
+// states of the two electron digits at one configuration of all other
+// spins) form a block row; H[quartet q, quartet q'] is a 4x4 complex block.
+// For radical pairs a block row has 1 + (number of nuclear flips) blocks
+// (13 at D=16384 instead of 27 scalars per row), and each gathered quartet
+// feeds all four output rows from registers.  Blocks are typed by their
+// sparsity so the inner product only touches structural nonzeros.
+//
+// Compact quartet form: per block an int2 {base row << 3 | type, value
+// offset}; values are complex64, two per float4 (offset counted in float4),
+// and hold only what the type needs:
+//   0 full 4x4 (16, row-major in the pair index a = 2*a1 + a2)
+//   1 acts on digit 1 with a2 == b2: 8 values [a2][a1][b1]
+//   2 acts on digit 2 with a1 == b1: 8 values [a1][a2][b2]
+//   3 diagonal: 4 values [a]
+//   4 A (x) I on digit 1: 4 values [a1][b1]
+//   5 I (x) A on digit 2: 4 values [a2][b2]
+// A hyperfine flip block S_e.A.I_n is type 4 or 5: 4 values instead of 16.
+struct QuartetC {
+    const int *rowptr;  // Q + 1
+    const int2 *blk;    // nblocks
+    const float4 *val;  // value pairs
+    const int *base;    // Q
+};
+
+// Complex64 vectors are stored "pair-planar": the 16 bytes of trajectories
+// (t, t+1), t even, hold {re(t), re(t+1), im(t), im(t+1)}.  One complex
+// multiply-accumulate of a scalar b into both trajectories is then four
+// packed FP32x2 FMAs (Blackwell FFMA2) on the re and im pairs.  Matrix values
+// stay compact (two complex values per 16-byte load); they are broadcast into
+// pairs in registers.
+__device__ __forceinline__ void mac_pp(float2 o[2], float br_, float bi_, float4 x)
+{
+    const float2 br = make_float2(br_, br_), bi = make_float2(bi_, bi_), nbi = make_float2(-bi_, -bi_);
+    const float2 re = make_float2(x.x, x.y), im = make_float2(x.z, x.w);
+    o[0] = __ffma2_rn(br, re, o[0]);
+    o[0] = __ffma2_rn(nbi, im, o[0]);
+    o[1] = __ffma2_rn(br, im, o[1]);
+    o[1] = __ffma2_rn(bi, re, o[1]);
+}
+
+// o[a] = {re pair, im pair} of output row a; v = the block's values, two
+// complex values per float4 in the storage order of the type.
+__device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const float4 *__restrict__ v,
+                                              const float4 x[4])
+{
+    switch (type) {
+    case 0:
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float4 p = __ldg(v + 2 * a), q = __ldg(v + 2 * a + 1);
+            mac_pp(o[a], p.x, p.y, x[0]);
+            mac_pp(o[a], p.z, p.w, x[1]);
+            mac_pp(o[a], q.x, q.y, x[2]);
+            mac_pp(o[a], q.z, q.w, x[3]);
+        }
+        break;
+    case 1:
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2)
+#pragma unroll
+            for (int a1 = 0; a1 < 2; ++a1) {
+                const float4 p = __ldg(v + 2 * a2 + a1);
+                mac_pp(o[2 * a1 + a2], p.x, p.y, x[a2]);
+                mac_pp(o[2 * a1 + a2], p.z, p.w, x[2 + a2]);
+            }
+        break;
+    case 2:
+#pragma unroll
+        for (int a1 = 0; a1 < 2; ++a1)
+#pragma unroll
+            for (int a2 = 0; a2 < 2; ++a2) {
+                const float4 p = __ldg(v + 2 * a1 + a2);
+                mac_pp(o[2 * a1 + a2], p.x, p.y, x[2 * a1]);
+                mac_pp(o[2 * a1 + a2], p.z, p.w, x[2 * a1 + 1]);
+            }
+        break;
+    case 3: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);
+        mac_pp(o[0], p.x, p.y, x[0]);
+        mac_pp(o[1], p.z, p.w, x[1]);
+        mac_pp(o[2], q.x, q.y, x[2]);
+        mac_pp(o[3], q.z, q.w, x[3]);
+        break;
+    }
+    case 4: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);  // A00 A01 | A10 A11
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+            mac_pp(o[a2], p.x, p.y, x[a2]);
+            mac_pp(o[a2], p.z, p.w, x[2 + a2]);
+            mac_pp(o[2 + a2], q.x, q.y, x[a2]);
+            mac_pp(o[2 + a2], q.z, q.w, x[2 + a2]);
+        }
+        break;
+    }
+    default: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);
+#pragma unroll
+        for (int a1 = 0; a1 < 2; ++a1) {
+            mac_pp(o[2 * a1], p.x, p.y, x[2 * a1]);
+            mac_pp(o[2 * a1], p.z, p.w, x[2 * a1 + 1]);
+            mac_pp(o[2 * a1 + 1], q.x, q.y, x[2 * a1]);
+            mac_pp(o[2 * a1 + 1], q.z, q.w, x[2 * a1 + 1]);
+        }
+        break;
+    }
+    }
+}
+
+// U = H v_j over quartet tiles (QT quartets x 64 trajectories per CTA) with
+// the compact block form; the gathers of block k+1 are issued before the
+// arithmetic of block k.  Partial alpha_j = Re <v_j, U> in FP64.
+// kPrefetch: issue block k+1's gathers before block k's arithmetic (more
+// loads in flight, more registers); kMinBlocks: CTAs per SM the register
+// allocation must allow.  The autotuner picks the variant per shape.
+template <bool kPrefetch, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_lanczos_apply_compact(QuartetC H, const float2 *__restrict__ wj, const double *__restrict__ sj,
+                        float2 *__restrict__ U, double *__restrict__ part, int Q, int s1, int s2, int ldm, int QT)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = blockIdx.y * 64 + 2 * lane;
-    const int r0 = blockIdx.x * R;
-    const float s0 = static_cast<float>(sj[t]), s1 = static_cast<float>(sj[t + 1]);
+    const int q0 = blockIdx.x * QT;
+    const float sc0 = static_cast<float>(sj[t]), sc1 = static_cast<float>(sj[t + 1]);
+    const int off[4] = {0, s2, s1, s1 + s2};
     double a0 = 0.0, a1 = 0.0;
-    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
-        float2 acc0 = make_float2(0.f, 0.f), acc1 = make_float2(0.f, 0.f);
-        float2 cor0 = make_float2(0.f, 0.f), cor1 = make_float2(0.f, 0.f);
-        const int kb = __ldg(H.rowptr + r), ke = __ldg(H.rowptr + r + 1);
+    for (int q = q0 + warp; q < min(q0 + QT, Q); q += kWarps) {
+        float2 o[4][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) o[a][0] = o[a][1] = make_float2(0.f, 0.f);
+        const int kb = __ldg(H.rowptr + q), ke = __ldg(H.rowptr + q + 1);
+        int2 cur = __ldg(H.blk + kb);
+        float4 x[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            x[b] = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>((cur.x >> 3) + off[b]) * ldm + t);
         for (int k = kb; k < ke; ++k) {
-            const int c = __ldg(H.col + k);
-            const float2 h = __ldg(H.hi + k);
-            const float4 x = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>(c) * ldm + t);
-            acc0 = cfmaf(h, make_float2(x.x, x.y), acc0);
-            acc1 = cfmaf(h, make_float2(x.z, x.w), acc1);
-            if (kSplit) {
-                const float2 hl = __ldg(H.lo + k);
-                cor0 = cfmaf(hl, make_float2(x.x, x.y), cor0);
-                cor1 = cfmaf(hl, make_float2(x.z, x.w), cor1);
+            if (kPrefetch) {
+                int2 nxt = cur;
+                float4 xn[4];
+                if (k + 1 < ke) {
+                    nxt = __ldg(H.blk + k + 1);
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        xn[b] = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>((nxt.x >> 3) + off[b]) * ldm + t);
+                }
+                quartet_block(o, cur.x & 7, H.val + cur.y, x);
+                cur = nxt;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) x[b] = xn[b];
+            } else {
+                quartet_block(o, cur.x & 7, H.val + cur.y, x);
+                if (k + 1 < ke) {
+                    cur = __ldg(H.blk + k + 1);
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        x[b] = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>((cur.x >> 3) + off[b]) * ldm + t);
+                }
             }
         }
-        if (kSplit) {
-            acc0.x += cor0.x; acc0.y += cor0.y;
-            acc1.x += cor1.x; acc1.y += cor1.y;
+        const int base = __ldg(H.base + q);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const size_t e = static_cast<size_t>(base + off[a]) * ldm + t;
+            const float2 ure = make_float2(o[a][0].x * sc0, o[a][0].y * sc1);
+            const float2 uim = make_float2(o[a][1].x * sc0, o[a][1].y * sc1);
+            *reinterpret_cast<float4 *>(U + e) = make_float4(ure.x, ure.y, uim.x, uim.y);
+            const float4 v = *reinterpret_cast<const float4 *>(wj + e);  // {re t, re t+1, im t, im t+1}
+            a0 += (static_cast<double>(v.x) * ure.x + static_cast<double>(v.z) * uim.x) * sc0;
+            a1 += (static_cast<double>(v.y) * ure.y + static_cast<double>(v.w) * uim.y) * sc1;
         }
-        acc0.x *= s0; acc0.y *= s0; acc1.x *= s1; acc1.y *= s1;
-        const size_t e = static_cast<size_t>(r) * ldm + t;
-        const float4 v = *reinterpret_cast<const float4 *>(wj + e);
-        *reinterpret_cast<float4 *>(U + e) = make_float4(acc0.x, acc0.y, acc1.x, acc1.y);
-        a0 += (static_cast<double>(v.x) * acc0.x + static_cast<double>(v.y) * acc0.y) * s0;
-        a1 += (static_cast<double>(v.z) * acc1.x + static_cast<double>(v.w) * acc1.y) * s1;
     }
     __shared__ double sm[kWarps][64];
     sm[warp][2 * lane] = a0;
@@ -247,17 +390,18 @@ k_lanczos_update(const float2 *__restrict__ U, const float2 *__restrict__ wj, co
         const size_t e = static_cast<size_t>(r) * ldm + t;
         const float4 u = *reinterpret_cast<const float4 *>(U + e);
         const float4 v = *reinterpret_cast<const float4 *>(wj + e);
+        // pair-planar {re t, re t+1, im t, im t+1}
         float4 o;
-        o.x = fmaf(-ca0, v.x, u.x); o.y = fmaf(-ca0, v.y, u.y);
-        o.z = fmaf(-ca1, v.z, u.z); o.w = fmaf(-ca1, v.w, u.w);
+        o.x = fmaf(-ca0, v.x, u.x); o.y = fmaf(-ca1, v.y, u.y);
+        o.z = fmaf(-ca0, v.z, u.z); o.w = fmaf(-ca1, v.w, u.w);
         if (wjm1) {
             const float4 p = *reinterpret_cast<const float4 *>(wjm1 + e);
-            o.x = fmaf(-cb0, p.x, o.x); o.y = fmaf(-cb0, p.y, o.y);
-            o.z = fmaf(-cb1, p.z, o.z); o.w = fmaf(-cb1, p.w, o.w);
+            o.x = fmaf(-cb0, p.x, o.x); o.y = fmaf(-cb1, p.y, o.y);
+            o.z = fmaf(-cb0, p.z, o.z); o.w = fmaf(-cb1, p.w, o.w);
         }
         *reinterpret_cast<float4 *>(wn + e) = o;
-        n0 += static_cast<double>(o.x) * o.x + static_cast<double>(o.y) * o.y;
-        n1 += static_cast<double>(o.z) * o.z + static_cast<double>(o.w) * o.w;
+        n0 += static_cast<double>(o.x) * o.x + static_cast<double>(o.z) * o.z;
+        n1 += static_cast<double>(o.y) * o.y + static_cast<double>(o.w) * o.w;
     }
     __shared__ double sm[kWarps][64];
     sm[warp][2 * lane] = n0;
@@ -273,14 +417,22 @@ k_lanczos_update(const float2 *__restrict__ U, const float2 *__restrict__ wj, co
 // out[t] = sum over tiles of part[tile][t] (fixed order), optional sqrt and
 // Lanczos bookkeeping: mode 0 -> alpha_j (stored to T diag), mode 1 -> beta_{j+1}
 // (stored to T offdiag, scale = 1/beta, breakdown marks the dimension).
+// Launch with blockDim (32, 8) and ldm/32 blocks: thread (x, y) sums tiles
+// y, y+8, ... of trajectory t, then the 8 column sums are added in order.
 __global__ void k_lanczos_reduce(const double *__restrict__ part, int ntiles, int ldm, int mode, int j, int m,
                                  double *__restrict__ out, double *__restrict__ tdiag, double *__restrict__ toff,
                                  int *__restrict__ mdim)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ldm) return;
+    __shared__ double red[8][33];
+    const int t = blockIdx.x * 32 + threadIdx.x;
+    double ps = 0.0;
+    for (int tile = threadIdx.y; tile < ntiles; tile += 8) ps += part[static_cast<size_t>(tile) * ldm + t];
+    red[threadIdx.y][threadIdx.x] = ps;
+    __syncthreads();
+    if (threadIdx.y != 0) return;
     double s = 0.0;
-    for (int tile = 0; tile < ntiles; ++tile) s += part[static_cast<size_t>(tile) * ldm + t];
+#pragma unroll
+    for (int y = 0; y < 8; ++y) s += red[y][threadIdx.x];
     const bool active = mdim[t] == 0;
     if (mode == 0) {
         out[t] = s;
@@ -339,7 +491,7 @@ __global__ void k_krylov_expm(const double2 *__restrict__ hess, const double *__
             c = cscale(y[lane], b0);
             if (vscale) c = cscale(c, vscale[static_cast<size_t>(lane) * ldm + t]);
         }
-        coef[static_cast<size_t>(t) * m + lane] = c;
+        coef[static_cast<size_t>(lane) * ldm + t] = c;
     }
     if (!ok && lane == 0 && t < M) atomicOr(status, 1);
 }
@@ -432,7 +584,7 @@ k_combine(T *__restrict__ psi, const T *__restrict__ V, size_t vstride, const do
 #pragma unroll
             for (int a = 0; a < 4; ++a) x[a] = make_double2(0.0, 0.0);
             for (int jj = 0; jj < n; ++jj) {
-                const double2 c = coef[static_cast<size_t>(t) * m + jj];
+                const double2 c = coef[static_cast<size_t>(jj) * ldm + t];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const T v = V[jj * vstride + e[a]];
@@ -466,6 +618,107 @@ k_combine(T *__restrict__ psi, const T *__restrict__ V, size_t vstride, const do
         for (int w = 0; w < blockDim.y; ++w) s += sm[8][w][threadIdx.x];
         part_nrm[static_cast<size_t>(blockIdx.x) * ldm + t] = s;
     }
+}
+
+// Pair-planar complex64 form of k_combine: each thread owns a trajectory pair
+// (t, t+1) of a quartet (16-byte loads).  blockDim = (32, 8): x over 32
+// pairs (64 trajectories), y over quartets of the tile.
+template <bool kBasis>
+__global__ void __launch_bounds__(256)
+k_combine_pp(float2 *__restrict__ psi, const float2 *__restrict__ V, size_t vstride, const double2 *__restrict__ coef,
+             const int *__restrict__ mdim, int s1, int s2, int Q, int ldm, int QR, Noise nz, long long stepA, int halfA,
+             double pA, long long stepB, int halfB, double pB, PairObs po, double *__restrict__ part_obs,
+             double *__restrict__ part_nrm)
+{
+    const int t = blockIdx.y * 64 + 2 * threadIdx.x;
+    const int q0 = blockIdx.x * QR;
+    double obs[2][8] = {{0, 0, 0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0, 0, 0}};
+    double nrm[2] = {0.0, 0.0};
+    int n = 0;
+    if (kBasis) n = max(max(1, mdim[t]), max(1, mdim[t + 1]));
+    int flip[2];
+    for (int k = 0; k < 2; ++k) {
+        flip[k] = noise_bit(nz, t + k, stepA, halfA, pA);
+        if (stepB >= 0) flip[k] ^= noise_bit(nz, t + k, stepB, halfB, pB);
+    }
+    for (int q = q0 + threadIdx.y; q < min(q0 + QR, Q); q += blockDim.y) {
+        const int base = quartet_base(q, s1, s2);
+        size_t e[4];
+        e[0] = static_cast<size_t>(base) * ldm + t;
+        e[1] = static_cast<size_t>(base + s2) * ldm + t;
+        e[2] = static_cast<size_t>(base + s1) * ldm + t;
+        e[3] = static_cast<size_t>(base + s1 + s2) * ldm + t;
+        double2 x[2][4];
+        if (kBasis) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) x[0][a] = x[1][a] = make_double2(0.0, 0.0);
+#pragma unroll 4
+            for (int jj = 0; jj < n; ++jj) {
+                // coefficients are zero beyond a trajectory's own Krylov dimension
+                const double2 c0 = coef[static_cast<size_t>(jj) * ldm + t];
+                const double2 c1 = coef[static_cast<size_t>(jj) * ldm + t + 1];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const float4 v = *reinterpret_cast<const float4 *>(V + jj * vstride + e[a]);
+                    x[0][a] = cfma(c0, make_double2(v.x, v.z), x[0][a]);
+                    x[1][a] = cfma(c1, make_double2(v.y, v.w), x[1][a]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const float4 v = *reinterpret_cast<const float4 *>(psi + e[a]);
+                x[0][a] = make_double2(v.x, v.z);
+                x[1][a] = make_double2(v.y, v.w);
+            }
+        }
+        quartet_epilogue(x[0], flip[0], po, obs[0], nrm[0]);
+        quartet_epilogue(x[1], flip[1], po, obs[1], nrm[1]);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            *reinterpret_cast<float4 *>(psi + e[a]) =
+                make_float4(static_cast<float>(x[0][a].x), static_cast<float>(x[1][a].x),
+                            static_cast<float>(x[0][a].y), static_cast<float>(x[1][a].y));
+    }
+    __shared__ double sm[9][8][65];
+    for (int o = 0; o < po.nobs; ++o) {
+        sm[o][threadIdx.y][2 * threadIdx.x] = obs[0][o];
+        sm[o][threadIdx.y][2 * threadIdx.x + 1] = obs[1][o];
+    }
+    sm[8][threadIdx.y][2 * threadIdx.x] = nrm[0];
+    sm[8][threadIdx.y][2 * threadIdx.x + 1] = nrm[1];
+    __syncthreads();
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid < 64) {
+        const int tt = blockIdx.y * 64 + tid;
+        for (int o = 0; o < po.nobs; ++o) {
+            double s = 0.0;
+            for (int w = 0; w < blockDim.y; ++w) s += sm[o][w][tid];
+            part_obs[(static_cast<size_t>(blockIdx.x) * po.nobs + o) * ldm + tt] = s;
+        }
+        double s = 0.0;
+        for (int w = 0; w < blockDim.y; ++w) s += sm[8][w][tid];
+        part_nrm[static_cast<size_t>(blockIdx.x) * ldm + tt] = s;
+    }
+}
+
+// complex128 interleaved <-> complex64 pair-planar (n = D * ldm elements)
+__global__ void k_c128_to_pp(float4 *__restrict__ out, const double2 *__restrict__ in, size_t npairs)
+{
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= npairs) return;
+    const double2 a = in[2 * i], b = in[2 * i + 1];
+    out[i] = make_float4(static_cast<float>(a.x), static_cast<float>(b.x), static_cast<float>(a.y),
+                         static_cast<float>(b.y));
+}
+
+__global__ void k_pp_to_c128(double2 *__restrict__ out, const float4 *__restrict__ in, size_t npairs)
+{
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= npairs) return;
+    const float4 v = in[i];
+    out[2 * i] = make_double2(v.x, v.z);
+    out[2 * i + 1] = make_double2(v.y, v.w);
 }
 
 // Per-trajectory trapezoid accumulation (compensated) of the observable
