@@ -53,6 +53,14 @@ extern "C" {
 /* Propagators. */
 #define MSGPU_PROP_KRYLOV 0
 
+/* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
+ * dimensions (the whole time loop in one launch, one warp per trajectory,
+ * Krylov basis in shared memory) and STREAMED otherwise (one kernel sequence
+ * per step over the trajectory block, vectors in HBM). */
+#define MSGPU_FORM_AUTO 0
+#define MSGPU_FORM_STREAMED 1
+#define MSGPU_FORM_RESIDENT 2
+
 /* Noise modes for the singlet-triplet dephasing Operator. */
 #define MSGPU_NOISE_NONE 0
 #define MSGPU_NOISE_REPLAY 1 /* host-supplied flip bits (e.g. the reference's mt19937 stream) */
@@ -133,6 +141,10 @@ int msgpu_fetch_values(msgpu_ctx *ctx, double *values);
  * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield. */
 int msgpu_profile_enable(msgpu_ctx *ctx, int enable);
 int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long long *launches);
+
+/* Select the execution form (MSGPU_FORM_*); RESIDENT falls back to an error
+ * at run time if the Krylov basis of one trajectory does not fit shared memory. */
+int msgpu_set_form(msgpu_ctx *ctx, int form);
 
 /* Number of kernels this context launched since creation. */
 long long msgpu_launch_count(const msgpu_ctx *ctx);

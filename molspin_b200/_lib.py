@@ -32,6 +32,9 @@ PROP_KRYLOV = 0
 NOISE_NONE = 0
 NOISE_REPLAY = 1
 NOISE_PHILOX = 2
+FORM_AUTO = 0
+FORM_STREAMED = 1
+FORM_RESIDENT = 2
 
 KC_APPLY, KC_ORTH, KC_REDUCE, KC_EXPM, KC_COMBINE, KC_YIELD = range(6)
 
@@ -83,6 +86,7 @@ def _load() -> C.CDLL:
         "msgpu_profile_enable": (I, [P, I]),
         "msgpu_profile_read": (I, [P, I, pD, C.POINTER(C.c_longlong)]),
         "msgpu_launch_count": (C.c_longlong, [P]),
+        "msgpu_set_form": (I, [P, I]),
         "msgpu_krylov_step_noalloc": (I, [I, P, P, P, D, I, P, P, D, I, P]),
         "msgpu_host_build_hamiltonian": (C.c_longlong, [I, pI, I, pI, pD, I, pI, pI, pD, pI, pI, pD]),
         "msgpu_host_trace_samples": (I, [D, pD, I, I, I, pD]),

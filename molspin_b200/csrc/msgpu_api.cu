@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "msgpu_kernels.cuh"
+#include "msgpu_resident.cuh"
 
 using namespace msgpu;
 
@@ -45,6 +46,9 @@ struct msgpu_ctx {
     int q_s1 = 0, q_s2 = 0, q_D = 0, q_nblocks = 0;
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
     int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
+    // resident (one warp per trajectory, whole time loop per launch) form
+    int form = MSGPU_FORM_AUTO;
+    DevBuf colbuf, trajval, times_d, pflip_d, sys_d, work_d, obs_d;
     // reaction
     bool k_scalar = true;
     double kappa = 0.0;
@@ -223,7 +227,8 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->krow, &c->kcol, &c->kval, &c->bits,
                      &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
-                     &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d};
+                     &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
+                     &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d};
     for (DevBuf *b : all) release(c, *b);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -234,6 +239,14 @@ const char *msgpu_last_error(const msgpu_ctx *c) { return c ? c->err.c_str() : "
 size_t msgpu_device_bytes(const msgpu_ctx *c) { return c ? c->used : 0; }
 
 long long msgpu_launch_count(const msgpu_ctx *c) { return c ? c->launches : 0; }
+
+int msgpu_set_form(msgpu_ctx *c, int form)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (form < MSGPU_FORM_AUTO || form > MSGPU_FORM_RESIDENT) return fail(c, MSGPU_ERR_INVALID, "unknown form");
+    c->form = form;
+    return MSGPU_OK;
+}
 
 int msgpu_set_stream(msgpu_ctx *c, void *s)
 {
@@ -517,6 +530,158 @@ int ensure_state(msgpu_ctx *c, int prec)
 
 double flip_p(double st_rate, double h) { return -0.5 * std::expm1(-2.0 * (0.5 * st_rate) * h); }
 
+// Warps per CTA of the resident form for this problem, 0 if it does not
+// apply (streamed form forced, dimension too large for the shared-memory
+// basis, Lanczos asked for with a non-scalar K).
+constexpr size_t kResidentSmemBudget = 200 * 1024;
+constexpr int kResidentMaxDim = 1024;
+
+int resident_warps(const msgpu_ctx *c, int prec, int m)
+{
+    if (c->form == MSGPU_FORM_STREAMED) return 0;
+    if (prec == MSGPU_PREC_C64 && !c->k_scalar) return 0;
+    if (c->form == MSGPU_FORM_AUTO && c->D > kResidentMaxDim) return 0;
+    const size_t wb = resident_warp_bytes(c->D, m, prec == MSGPU_PREC_C128 ? 16 : 8);
+    const int w = static_cast<int>(std::min<size_t>(4, kResidentSmemBudget / wb));
+    return w;
+}
+
+int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
+{
+    const int D = c->D, ldm = c->ldm, M = c->M;
+    const int nobs = static_cast<int>(c->obs.size());
+    const int warps = resident_warps(c, prec, m);
+    const size_t wb = resident_warp_bytes(D, m, prec == MSGPU_PREC_C128 ? 16 : 8);
+    cudaStream_t st = c->stream;
+    int rc;
+    if ((rc = ensure_state(c, MSGPU_PREC_C128)) ||
+        (rc = ensure(c, c->colbuf, static_cast<size_t>(D) * M * sizeof(double2), "resident state")) ||
+        (rc = ensure(c, c->acc, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield acc")) ||
+        (rc = ensure(c, c->comp, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield comp")) ||
+        (rc = ensure(c, c->prev, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield prev")) ||
+        (rc = ensure(c, c->rates_d, 8 * sizeof(double), "rates")) ||
+        (rc = ensure(c, c->status, sizeof(int), "status")) ||
+        (rc = ensure(c, c->values_d, static_cast<size_t>(p->ntimes) * nobs * sizeof(double), "values")) ||
+        (rc = ensure(c, c->trajval, static_cast<size_t>(p->ntimes) * M * nobs * sizeof(double), "values per trajectory")) ||
+        (rc = ensure(c, c->times_d, static_cast<size_t>(p->ntimes) * sizeof(double), "times")) ||
+        (rc = ensure(c, c->pflip_d, static_cast<size_t>(p->ntimes) * sizeof(double), "flip probabilities")) ||
+        (rc = ensure(c, c->sys_d, sizeof(ResidentSystem), "system")) ||
+        (rc = ensure(c, c->work_d, static_cast<size_t>(M) * sizeof(ResidentWork), "work list")) ||
+        (rc = ensure(c, c->obs_d, 8 * 16 * sizeof(double2), "observables")))
+        return rc;
+    // flip probabilities and observables in the kernel's pair basis
+    std::vector<double> pf(p->ntimes, 0.0);
+    for (int s = 0; s + 1 < p->ntimes; ++s) pf[s] = flip_p(c->st_rate, 0.5 * (p->times[s + 1] - p->times[s]));
+    const PairObs po = make_pair_obs(c);
+    std::vector<ResidentWork> work(M);
+    for (int t = 0; t < M; ++t) work[t] = ResidentWork{0, t};
+    ResidentSystem S;
+    std::memset(&S, 0, sizeof(S));
+    S.rowptr = static_cast<const int *>(c->hrow.p);
+    S.col = static_cast<const int *>(c->hcol.p);
+    S.val = static_cast<const double2 *>(c->hval.p);
+    S.valf = static_cast<const float2 *>(c->hhi.p);
+    if (!c->k_scalar) {
+        S.krow = static_cast<const int *>(c->krow.p);
+        S.kcol = static_cast<const int *>(c->kcol.p);
+        S.kval = static_cast<const double2 *>(c->kval.p);
+    }
+    S.kappa = c->k_scalar ? c->kappa : 0.0;
+    S.D = D;
+    S.M = M;
+    S.acc_ld = ldm;  // acc/comp/prev share the streamed layout [nobs][ldm]
+    S.m = m;
+    S.s1 = c->s1;
+    S.s2 = c->s2;
+    S.nobs = nobs;
+    S.obs = static_cast<const double2 *>(c->obs_d.p);
+    S.rates = static_cast<const double *>(c->rates_d.p);
+    S.nz.mode = c->noise_mode;
+    S.nz.bits = static_cast<const uint8_t *>(c->bits.p);
+    S.nz.bits_steps = c->bits_steps;
+    S.nz.M = c->noise_mode == MSGPU_NOISE_REPLAY ? c->bits_ntraj : M;
+    S.nz.seed = c->seed;
+    S.psi = c->colbuf.p;
+    S.acc = static_cast<double *>(c->acc.p);
+    S.comp = static_cast<double *>(c->comp.p);
+    S.prev = static_cast<double *>(c->prev.p);
+    S.traj_values = static_cast<double *>(c->trajval.p);
+    S.times = static_cast<const double *>(c->times_d.p);
+    S.pflip = static_cast<const double *>(c->pflip_d.p);
+    S.ntimes = p->ntimes;
+    S.step_offset = p->step_offset;
+    S.accumulate = p->accumulate;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->rates_d.p, c->rates.data(), nobs * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->obs_d.p, po.op, sizeof(double2) * 16 * nobs, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->times_d.p, p->times, sizeof(double) * p->ntimes, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->pflip_d.p, pf.data(), sizeof(double) * p->ntimes, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->sys_d.p, &S, sizeof(S), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->work_d.p, work.data(), sizeof(ResidentWork) * M, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemsetAsync(c->status.p, 0, sizeof(int), st)))
+        return cuda_fail(c, e, "resident setup");
+    // column-major state for the warps (complex64: narrowed through zbuf)
+    const size_t ne = static_cast<size_t>(D) * M;
+    double2 *col128 = static_cast<double2 *>(c->colbuf.p);
+    if (prec == MSGPU_PREC_C64)
+        if (int rc2 = ensure(c, c->zbuf, ne * sizeof(double2), "resident staging")) return rc2;
+    double2 *stage = prec == MSGPU_PREC_C64 ? static_cast<double2 *>(c->zbuf.p) : col128;
+    {
+        Timed tm(c, KC_COMBINE);
+        dim3 grid(ceil_div(D, 32), ldm / 32), block(32, 8);
+        k_interleaved_to_cols<double2><<<grid, block, 0, st>>>(stage, static_cast<const double2 *>(c->psi128.p), D, M, ldm);
+        if (prec == MSGPU_PREC_C64)
+            k_convert<float2, double2><<<ceil_div(ne, 256), 256, 0, st>>>(reinterpret_cast<float2 *>(col128), stage, ne);
+    }
+    const size_t smem = static_cast<size_t>(warps) * wb;
+    const int blocks = ceil_div(M, warps);
+    {
+        Timed tm(c, KC_APPLY);
+        if (prec == MSGPU_PREC_C128) {
+            if ((e = cudaFuncSetAttribute(k_resident<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem))))
+                return cuda_fail(c, e, "resident shared memory");
+            k_resident<double2, false><<<blocks, 32 * warps, smem, st>>>(
+                static_cast<const ResidentSystem *>(c->sys_d.p), static_cast<const ResidentWork *>(c->work_d.p), M, wb,
+                static_cast<int *>(c->status.p));
+        } else {
+            if ((e = cudaFuncSetAttribute(k_resident<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem))))
+                return cuda_fail(c, e, "resident shared memory");
+            k_resident<float2, true><<<blocks, 32 * warps, smem, st>>>(
+                static_cast<const ResidentSystem *>(c->sys_d.p), static_cast<const ResidentWork *>(c->work_d.p), M, wb,
+                static_cast<int *>(c->status.p));
+        }
+    }
+    {
+        Timed tm(c, KC_YIELD);
+        k_resident_values<<<p->ntimes, 256, 0, st>>>(static_cast<const double *>(c->trajval.p), M, nobs,
+                                                      static_cast<double *>(c->values_d.p));
+    }
+    {
+        Timed tm(c, KC_COMBINE);
+        if (prec == MSGPU_PREC_C64)
+            k_convert<double2, float2><<<ceil_div(ne, 256), 256, 0, st>>>(stage, reinterpret_cast<const float2 *>(col128), ne);
+        dim3 grid(ceil_div(D, 32), ldm / 32), block(32, 8);
+        k_cols_to_interleaved<double2><<<grid, block, 0, st>>>(static_cast<double2 *>(c->psi128.p), stage, D, M, ldm);
+    }
+    int status = 0;
+    c->last_values.assign(static_cast<size_t>(p->ntimes) * nobs, 0.0);
+    if ((e = cudaGetLastError()) ||
+        (e = cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(c->last_values.data(), c->values_d.p, c->last_values.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+        return cuda_fail(c, e, "resident run");
+    collect_profile(c);
+    c->state_prec = MSGPU_PREC_C128;
+    c->last_ntimes = p->ntimes;
+    c->have_integrals = true;
+    if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite observable or norm on the device");
+    if (status & 1) return fail(c, MSGPU_ERR_EXPM, "run: small matrix exponential failed");
+    return MSGPU_OK;
+}
+
 // Quartet-block form of H for the current electron strides (see QuartetC).
 int build_quartet(msgpu_ctx *c)
 {
@@ -748,6 +913,9 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     const int D = c->D, ldm = c->ldm, M = c->M;
     const int m = std::min(p->krylov_dim, D);
     const int prec = p->precision;
+    if (resident_warps(c, prec, m) > 0) return run_resident(c, p, prec, m);
+    if (c->form == MSGPU_FORM_RESIDENT)
+        return fail(c, MSGPU_ERR_INVALID, "run: the resident form does not fit this dimension / recurrence");
     const int nobs = static_cast<int>(c->obs.size());
     const size_t n = static_cast<size_t>(D) * ldm;
     // The complex64 state lives in slot 0 of the Lanczos basis: park it in the

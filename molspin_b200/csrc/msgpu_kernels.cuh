@@ -472,7 +472,8 @@ __global__ void k_krylov_expm(const double2 *__restrict__ hess, const double *__
         for (int i = 0; i < n; ++i) {
             double2 v;
             if (hess) {
-                v = hess[static_cast<size_t>(t) * m * m + i + lane * m];
+                // upper Hessenberg part only; entries below the subdiagonal are never written
+                v = i <= lane + 1 ? hess[static_cast<size_t>(t) * m * m + i + lane * m] : make_double2(0.0, 0.0);
             } else {
                 v = make_double2(0.0, 0.0);
                 if (i == lane) v = make_double2(-kappa, -tdiag[static_cast<size_t>(t) * m + i]);

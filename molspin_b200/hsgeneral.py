@@ -170,6 +170,11 @@ class HSPropagatorB200:
         _check(self.ctx, L.lib.msgpu_fetch_values(self.ctx, L.dptr(v)))
         return v
 
+    def set_form(self, form: str | int):
+        """"auto" | "streamed" | "resident" (see MSGPU_FORM_* in include/msgpu.h)."""
+        codes = {"auto": L.FORM_AUTO, "streamed": L.FORM_STREAMED, "resident": L.FORM_RESIDENT}
+        _check(self.ctx, L.lib.msgpu_set_form(self.ctx, codes[form] if isinstance(form, str) else int(form)))
+
     def launch_count(self) -> int:
         return int(L.lib.msgpu_launch_count(self.ctx))
 

@@ -20,9 +20,13 @@ from tests import helpers as h
 pytestmark = pytest.mark.gpu
 
 
+FORMS = ["streamed", "resident"]
+
+
 def _gpu(system, factors, times, krylov, precision="c128", noise=None, K_csr=None, kappa=None,
-         obs=None, chunks=None):
+         obs=None, chunks=None, form="auto"):
     with hs.HSPropagatorB200(0) as p:
+        p.set_form(form)
         p.set_hamiltonian(*system.hamiltonian_csr())
         if K_csr is not None:
             p.set_reaction(csr=K_csr)
@@ -61,12 +65,13 @@ def _rel(a, b):
     return np.max(np.abs(a - b)) / np.max(np.abs(b))
 
 
-def test_plain_per_trajectory_parity_config1_shape():
+@pytest.mark.parametrize("form", FORMS)
+def test_plain_per_trajectory_parity_config1_shape(form):
     w = S.plain_small()
     M, steps = 64, 200
     times = S.time_grid(steps * w.dt, w.dt)
     F = w.system.trace_samples(M, w.seed)
-    per, ens, values, Fg = _gpu(w.system, F, times, w.krylov)
+    per, ens, values, Fg = _gpu(w.system, F, times, w.krylov, form=form)
     ref = _oracle(w.system, F, times, w.krylov, kappa=w.system.kappa())
     assert _rel(per, ref["traj_yield"]) < 1e-10
     assert _rel(ens, ref["yield"]) < 1e-10
@@ -74,30 +79,34 @@ def test_plain_per_trajectory_parity_config1_shape():
     assert np.max(np.abs(Fg - ref["factors"])) < 1e-10 * np.max(np.abs(ref["factors"]))
 
 
-def test_plain_parity_reference_noise_stream():
+@pytest.mark.parametrize("form", FORMS)
+def test_plain_parity_reference_noise_stream(form):
     system = h.random_system([2, 2, 2], [2], seed=11, st_rate=0.05, sink=2e-3, hf_scale=3.0)
     M, times = 100, S.time_grid(60.0, 0.5)
     F = system.trace_samples(M, 7.0)
     bits = hs.reference_flip_bits(7.0, system.st_rate, times, M, orientation=0)
     assert np.unpackbits(bits).sum() > 50
-    per, ens, _, _ = _gpu(system, F, times, 12, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
+    per, ens, _, _ = _gpu(system, F, times, 12, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M),
+                          form=form)
     ref = _oracle(system, F, times, 12, U=True, kappa=system.kappa(), noise_mode=0, seed=7.0, seed_mode=0)
     assert _rel(per, ref["traj_yield"]) < 1e-10
     assert _rel(ens, ref["yield"]) < 1e-10
 
 
-def test_plain_parity_philox_replayed_on_cpu():
+@pytest.mark.parametrize("form", FORMS)
+def test_plain_parity_philox_replayed_on_cpu(form):
     system = h.random_system([2, 3], [2, 2], seed=12, st_rate=0.08, hf_scale=3.0)
     M, times = 70, S.time_grid(40.0, 1.0)
     F = system.trace_samples(M, 3.0)
     seed = 0xDEADBEEF1234
-    per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_PHILOX, seed))
+    per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_PHILOX, seed), form=form)
     bits = hs.philox_flip_bits(seed, system.st_rate, times, M)
     ref = _oracle(system, F, times, 16, U=True, kappa=system.kappa(), noise_mode=1, flip_bits=bits)
     assert _rel(per, ref["traj_yield"]) < 1e-10
 
 
-def test_plain_parity_general_K_and_interleaved_electrons():
+@pytest.mark.parametrize("form", FORMS)
+def test_plain_parity_general_K_and_interleaved_electrons(form):
     # electrons at positions 1 and 3 (neither leading), unequal sinks -> CSR K
     s = S.SpinSystem(mult=[2, 2, 3, 2, 2], names=["N1", "E1", "N2", "E2", "N3"], electrons=(1, 3))
     rng = np.random.default_rng(4)
@@ -114,16 +123,17 @@ def test_plain_parity_general_K_and_interleaved_electrons():
     F /= np.linalg.norm(F, axis=0) * math.sqrt(M)
     times = S.time_grid(30.0, 1.0)
     obs = [(op, rate) for _, op, rate in s.observables()]
-    per, ens, _, _ = _gpu(s, F, times, 10, K_csr=Kc, obs=obs)
+    per, ens, _, _ = _gpu(s, F, times, 10, K_csr=Kc, obs=obs, form=form)
     ref = orc.hs_stochastic(s.hamiltonian_csr(), F, times, h.oracle_observables(s), K_csr=Kc, krylov=10)
     assert _rel(per, ref["traj_yield"]) < 1e-10
 
 
-def test_exact_trace_against_density_oracle():
+@pytest.mark.parametrize("form", FORMS)
+def test_exact_trace_against_density_oracle(form):
     system = h.random_system([2, 2], [2], seed=21, hf_scale=2.0)
     times = S.time_grid(80.0, 1.0)
     F = den.orthonormal_nuclear_samples(system, S.SINGLET)
-    _, ens, values, _ = _gpu(system, F, times, 16)
+    _, ens, values, _ = _gpu(system, F, times, 16, form=form)
     H = den.dense_hamiltonian(system)
     K = system.kappa() * np.eye(system.dim)
     ops = [(den.pair_operator(op, system), rate) for _, op, rate in system.observables()]
@@ -151,15 +161,28 @@ def test_stochastic_st_against_lindblad_and_survival():
     assert np.max(np.abs(values - direct)) < h.six_sigma(M)
 
 
-def test_chunked_run_is_bitwise_identical():
+@pytest.mark.parametrize("form", FORMS)
+def test_chunked_run_is_bitwise_identical(form):
     system = h.random_system([2, 2, 2], [2, 2], seed=31, st_rate=0.05, hf_scale=2.0)
     M, times = 64, S.time_grid(40.0, 1.0)
     F = system.trace_samples(M, 5.0)
     noise = (system.st_rate, L.NOISE_PHILOX, 99)
-    a = _gpu(system, F, times, 12, noise=noise)
-    b = _gpu(system, F, times, 12, noise=noise, chunks=[13, 27, 40])
+    a = _gpu(system, F, times, 12, noise=noise, form=form)
+    b = _gpu(system, F, times, 12, noise=noise, chunks=[13, 27, 40], form=form)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[2], b[2])
+
+
+def test_resident_precision_form_against_plain():
+    # complex64 Lanczos in shared memory vs the complex128 Arnoldi path
+    system = h.random_system([2, 2, 2, 2], [2, 2, 2], seed=41, st_rate=0.05, hf_scale=2.0)
+    M, times = 96, S.time_grid(100.0, 1.0)
+    F = system.trace_samples(M, 9.0)
+    noise = (system.st_rate, L.NOISE_PHILOX, 7)
+    per64, ens64, val64, _ = _gpu(system, F, times, 16, precision="c64", noise=noise, form="resident")
+    per128, ens128, val128, _ = _gpu(system, F, times, 16, precision="c128", noise=noise, form="resident")
+    assert abs(ens64[0] - ens128[0]) <= 1e-6 * abs(ens128[0])
+    assert np.max(np.abs(val64 - val128)) <= 1e-6 * np.max(np.abs(val128))
 
 
 def test_precision_form_against_plain():
