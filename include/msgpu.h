@@ -146,6 +146,33 @@ int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long 
  * at run time if the Krylov basis of one trajectory does not fit shared memory. */
 int msgpu_set_form(msgpu_ctx *ctx, int form);
 
+/* ---------------------------------------------------------------- batching
+ * Many spin systems of uneven dimension and trajectory count propagated by
+ * ONE persistent launch (replayed from a CUDA graph): the loop over
+ * orientations / field values / systems of a powder or sweep run
+ * (TaskHSGeneral.cpp:347 orientation loop, RunSection::Step sweeps) with each
+ * system's HSGeneral time loop inside the launch.  Precision form
+ * (complex64 vectors, FP64 reductions and yield sums), Lanczos recurrence,
+ * K = kappa I, Philox noise keyed by (seed, trajectory, step, half).
+ * Systems with dimension >= the team threshold get a whole CTA per
+ * trajectory, smaller ones a warp; msgpu_batch_tune picks the threshold and
+ * the persistent grid size by timing the batch itself. */
+typedef struct msgpu_batch msgpu_batch;
+msgpu_batch *msgpu_batch_create(int device, size_t hbm_budget_bytes);
+void msgpu_batch_destroy(msgpu_batch *batch);
+const char *msgpu_batch_last_error(const msgpu_batch *batch);
+/* Returns the system index (>= 0) or -MSGPU_ERR_*.  ops: nobs 4x4 pair
+ * observables (as msgpu_add_pair_observable), factors: dim x ntraj
+ * column-major complex (HSPreparedState factors). */
+int msgpu_batch_add_system(msgpu_batch *batch, int dim, const int *rowptr, const int *col, const double *val,
+                           double kappa, int stride1, int stride2, int nobs, const double *ops, const double *rates,
+                           double st_rate, unsigned long long seed, int ntraj, const double *factors);
+int msgpu_batch_tune(msgpu_batch *batch, const double *times, int ntimes, int krylov_dim);
+int msgpu_batch_run(msgpu_batch *batch, const double *times, int ntimes, int krylov_dim, long long step_offset,
+                    int accumulate);
+int msgpu_batch_fetch_yields(msgpu_batch *batch, int system, double *per_traj, double *ensemble);
+int msgpu_batch_stats(const msgpu_batch *batch, double *last_run_ms, int *team_threshold, int *ctas_per_sm);
+
 /* Number of kernels this context launched since creation. */
 long long msgpu_launch_count(const msgpu_ctx *ctx);
 

@@ -87,6 +87,14 @@ def _load() -> C.CDLL:
         "msgpu_profile_read": (I, [P, I, pD, C.POINTER(C.c_longlong)]),
         "msgpu_launch_count": (C.c_longlong, [P]),
         "msgpu_set_form": (I, [P, I]),
+        "msgpu_batch_create": (P, [I, C.c_size_t]),
+        "msgpu_batch_destroy": (None, [P]),
+        "msgpu_batch_last_error": (C.c_char_p, [P]),
+        "msgpu_batch_add_system": (I, [P, I, pI, pI, pD, D, I, I, I, pD, pD, D, C.c_ulonglong, I, pD]),
+        "msgpu_batch_tune": (I, [P, pD, I, I]),
+        "msgpu_batch_run": (I, [P, pD, I, I, C.c_longlong, I]),
+        "msgpu_batch_fetch_yields": (I, [P, I, pD, pD]),
+        "msgpu_batch_stats": (I, [P, pD, pI, pI]),
         "msgpu_krylov_step_noalloc": (I, [I, P, P, P, D, I, P, P, D, I, P]),
         "msgpu_host_build_hamiltonian": (C.c_longlong, [I, pI, I, pI, pD, I, pI, pI, pD, pI, pI, pD]),
         "msgpu_host_trace_samples": (I, [D, pD, I, I, I, pD]),

@@ -20,8 +20,11 @@
 #include "msgpu_device.cuh"
 
 namespace msgpu {
+// Kernels defined in these headers have internal linkage: every translation
+// unit that includes them gets its own copies.
+namespace {
 
-constexpr int kWarps = 8;            // warps per CTA in the row-tiled kernels
+constexpr int kWarps = 8;           // warps per CTA in the row-tiled kernels
 constexpr int kThreads = 32 * kWarps;
 constexpr int kMaxKrylov = 32;
 
@@ -831,4 +834,5 @@ __global__ void k_interleaved_to_cols(double2 *__restrict__ out, const Src *__re
     }
 }
 
+}  // namespace
 }  // namespace msgpu

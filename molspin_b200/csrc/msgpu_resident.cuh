@@ -22,6 +22,7 @@
 #include "msgpu_kernels.cuh"
 
 namespace msgpu {
+namespace {  // internal linkage (see msgpu_kernels.cuh)
 
 struct ResidentSystem {
     // H (rad/ns) as CSR; values complex128 and complex64 copies
@@ -338,4 +339,5 @@ __global__ void k_resident_values(const double *__restrict__ traj_values, int M,
     }
 }
 
+}  // namespace
 }  // namespace msgpu

@@ -217,14 +217,16 @@ def dense_tc(M: int = 4096, steps: int = 20000) -> Workload:
                     precision="c64", seed=3.0)
 
 
-def batching_systems(n: int = 64, seed: int = 4) -> list[Workload]:
-    """64 radical pairs: 4-10 I=1/2 plus 0-2 I=1 (dims 64..9216), iso a ~ U[-1,1] mT,
-    B ~ U[0,1] mT (random direction), M ~ U[64,1024], k ~ U[0.5,2]/us, dt=1 ns, 4000 steps, m=16."""
+def batching_systems(n: int = 64, seed: int = 4, steps: int = 4000) -> list[Workload]:
+    """64 radical pairs with 4-10 nuclei, 0-2 of them I=1 and the rest I=1/2
+    (dims 64..9216), iso a ~ U[-1,1] mT, |B| ~ U[0,1] mT (random direction),
+    M ~ U[64,1024], k ~ U[0.5,2]/us, dt=1 ns, 4000 steps, m=16 (reference default)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
-        nh = int(rng.integers(4, 11))
+        ntot = int(rng.integers(4, 11))
         nn = int(rng.integers(0, 3))
+        nh = ntot - nn
         nuc = [2] * nh + [3] * nn
         split = int(rng.integers(1, len(nuc) + 1)) if len(nuc) > 1 else len(nuc)
         na, nb = nuc[:split], nuc[split:]
@@ -236,7 +238,7 @@ def batching_systems(n: int = 64, seed: int = 4) -> list[Workload]:
         k = rng.uniform(0.5e-3, 2e-3)
         s = radical_pair(na, nb, ca, cb, B, sink_rate=k)
         M = int(rng.integers(64, 1025))
-        out.append(Workload(f"batch[{i}] D={s.dim} M={M}", s, M=M, dt=1.0, steps=4000, krylov=16,
+        out.append(Workload(f"batch[{i}] D={s.dim} M={M}", s, M=M, dt=1.0, steps=steps, krylov=16,
                             precision="c64", seed=float(i + 1)))
     return out
 

@@ -1,0 +1,65 @@
+"""Batching form (msgpu_batch_*): several systems of uneven dimension in one
+persistent launch, against the CPU oracle and against itself in other mixes.
+
+Tolerance: complex64 vectors with FP64 reductions -> per-trajectory yields
+within 1e-6 of the largest per-trajectory yield of the complex128 oracle.
+"""
+import numpy as np
+import pytest
+
+from molspin_b200 import batching as B
+from molspin_b200 import hsgeneral as hs
+from molspin_b200 import systems as S
+from oracle import pyoracle as orc
+from tests import helpers as h
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    a = h.random_system([2, 2], [], seed=51, st_rate=0.05, hf_scale=2.0, aniso=False)           # D = 16
+    b = h.random_system([2, 3], [2], seed=52, st_rate=0.02, hf_scale=2.0, aniso=False)          # D = 48
+    c = h.random_system([2, 2, 2, 2], [2, 2, 2], seed=53, st_rate=0.03, hf_scale=2.0, aniso=False)  # D = 512
+    return [(a, 40, 11), (b, 70, 12), (c, 33, 13)]
+
+
+def _run(entries, times, krylov, chunks=None, tune=False):
+    with B.BatchB200(0) as bt:
+        idx = [bt.add(s, s.trace_samples(M, float(seed)), seed) for s, M, seed in entries]
+        if tune:
+            bt.tune(times[:4], krylov)
+        if chunks is None:
+            bt.run(times, krylov)
+        else:
+            start = 0
+            for k, stop in enumerate(chunks):
+                bt.run(times[start:stop + 1], krylov, step_offset=start, accumulate=k > 0)
+                start = stop
+        return [bt.yields(i) for i in idx], bt.stats()
+
+
+def test_batch_matches_oracle():
+    entries = _systems()
+    times = S.time_grid(30.0, 1.0)
+    m = 12
+    out, stats = _run(entries, times, m, tune=True)
+    assert stats["team_threshold"] > 0
+    for (s, M, seed), (per, ens) in zip(entries, out):
+        F = s.trace_samples(M, float(seed))
+        bits = hs.philox_flip_bits(seed, s.st_rate, times, M)
+        ref = orc.hs_stochastic(s.hamiltonian_csr(), F, times, h.oracle_observables(s), kappa=s.kappa(), krylov=m,
+                                U_csr=orc.st_unitary(s.mult, 0, 1), event_rate=0.5 * s.st_rate, noise_mode=1,
+                                flip_bits=bits, nthreads=8)
+        scale = np.max(np.abs(ref["traj_yield"]))
+        assert np.max(np.abs(per - ref["traj_yield"])) <= 1e-6 * scale, s.dim
+
+
+def test_batch_result_independent_of_companions_and_chunks():
+    entries = _systems()
+    times = S.time_grid(20.0, 1.0)
+    alone, _ = _run(entries[2:], times, 10)
+    mixed, _ = _run(entries, times, 10)
+    np.testing.assert_array_equal(alone[0][0], mixed[2][0])
+    chunked, _ = _run(entries, times, 10, chunks=[7, 20])
+    for x, y in zip(mixed, chunked):
+        np.testing.assert_array_equal(x[0], y[0])
