@@ -243,12 +243,13 @@ def batching_systems(n: int = 64, seed: int = 4, steps: int = 4000) -> list[Work
     return out
 
 
-def serving_request(req_id: int, grid: np.ndarray | None = None) -> Workload:
+def serving_request(req_id: int, grid: np.ndarray | None = None, nuclei: tuple[int, int] = (6, 14),
+                    steps: int = 3000) -> Workload:
     """One serving request: 6-14 I=1/2 (D=256..65536), anisotropic tensors seeded
     by the request id, one orientation of a 200-point sphere grid at 50 uT,
     256 trajectories, ST dephasing 0.1/us, k = 1/us, 3 us at dt = 1 ns."""
     rng = np.random.default_rng(10_000 + req_id)
-    nh = int(rng.integers(6, 15))
+    nh = int(rng.integers(nuclei[0], nuclei[1] + 1))
     na = int(rng.integers(1, nh))
     ta = [_aniso_tensor(rng, 1.5) for _ in range(na)]
     tb = [_aniso_tensor(rng, 1.5) for _ in range(nh - na)]
@@ -256,7 +257,7 @@ def serving_request(req_id: int, grid: np.ndarray | None = None) -> Workload:
         grid = sphere_grid(200)
     d = grid[int(rng.integers(0, len(grid)))]
     s = radical_pair([2] * na, [2] * (nh - na), ta, tb, 50e-6 * d, sink_rate=1e-3, st_rate=1e-4)
-    return Workload(f"request {req_id} D={s.dim}", s, M=256, dt=1.0, steps=3000, krylov=16, precision="c64",
+    return Workload(f"request {req_id} D={s.dim}", s, M=256, dt=1.0, steps=steps, krylov=16, precision="c64",
                     seed=float(req_id + 1))
 
 

@@ -1,0 +1,84 @@
+"""Host logic of the serving engine without a GPU: admission against slots
+and the memory budget, first-fit order, arrival times and the summary."""
+import threading
+import time
+
+import numpy as np
+
+from molspin_b200 import serving as SV
+from molspin_b200 import systems as S
+
+
+class FakeEngine(SV.ServingEngine):
+    def __init__(self, *a, work_s=0.05, **k):
+        super().__init__(*a, **k)
+        self.work_s = work_s
+        self.active = 0
+        self.peak_active = 0
+        self.lock = threading.Lock()
+        self.started = []
+
+    def solve(self, req, budget=0):
+        with self.lock:
+            self.active += 1
+            self.peak_active = max(self.peak_active, self.active)
+            self.started.append(req.rid)
+        time.sleep(self.work_s)
+        with self.lock:
+            self.active -= 1
+        return np.array([float(req.rid)])
+
+
+def _reqs(n, arrivals, nuclei=(6, 7)):
+    return [SV.Request(i, float(arrivals[i]), S.serving_request(i, nuclei=nuclei, steps=10), seed=i) for i in range(n)]
+
+
+def test_slots_limit_concurrency_and_all_complete():
+    reqs = _reqs(10, np.zeros(10))
+    eng = FakeEngine(hbm_budget=1 << 40, slots=3)
+    res = eng.serve(reqs, realtime=False)
+    assert [r.yields[0] for r in res] == list(range(10))
+    assert eng.peak_active <= 3 and eng.max_concurrency == 3
+    s = SV.summarize(res)
+    assert s["completed"] == 10 and s["p99_latency_s"] >= s["p50_latency_s"] > 0
+
+
+def test_budget_first_fit():
+    reqs = _reqs(6, np.zeros(6))
+    sizes = [SV.footprint(r.workload) for r in reqs]
+    budget = max(sizes) + min(sizes)
+    eng = FakeEngine(hbm_budget=budget, slots=6)
+    res = eng.serve(reqs, realtime=False)
+    assert all(not r.error for r in res)
+    assert eng.peak_reserved <= budget
+    assert eng.max_concurrency >= 1
+
+
+def test_oversized_request_is_refused_others_run():
+    reqs = _reqs(3, np.zeros(3))
+    sizes = [SV.footprint(r.workload) for r in reqs]
+    eng = FakeEngine(hbm_budget=sorted(sizes)[1], slots=2)
+    res = eng.serve(reqs, realtime=False)
+    big = int(np.argmax(sizes))
+    assert res[big].error and all(not r.error for i, r in enumerate(res) if i != big)
+
+
+def test_realtime_arrivals_are_honoured():
+    arrivals = np.array([0.0, 0.15, 0.3])
+    reqs = _reqs(3, arrivals)
+    eng = FakeEngine(hbm_budget=1 << 40, slots=4, work_s=0.01)
+    res = eng.serve(reqs, realtime=True)
+    for r, a in zip(res, arrivals):
+        assert r.admitted >= a - 1e-3
+        assert r.latency < 0.1
+
+
+def test_poisson_arrivals_rate():
+    a = SV.poisson_arrivals(20000, 50.0, seed=1)
+    assert abs(len(a) / a[-1] - 50.0) < 2.0 and np.all(np.diff(a) > 0)
+
+
+def test_footprint_grows_with_dimension():
+    small = SV.footprint(S.serving_request(0, nuclei=(6, 6), steps=10))
+    big = SV.footprint(S.serving_request(0, nuclei=(12, 12), steps=10))
+    assert big > 10 * small
