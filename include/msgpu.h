@@ -52,6 +52,20 @@ extern "C" {
 
 /* Propagators. */
 #define MSGPU_PROP_KRYLOV 0
+/* Dense propagator for a static H of dimension <= 4096 (the reference's
+ * "normal" expmat branch, HSPropagator.cpp:92-100): U = expm(dt(-iH-K)) is
+ * built once in FP64 on the device and applied every step as a real
+ * interleaved GEMM on the tensor cores (tcgen05, BF16 split operands, FP32
+ * accumulation).  Precision must be MSGPU_PREC_BF16X3 (two-part split, three
+ * products) or MSGPU_PREC_BF16X6 (three-part split, six products). */
+#define MSGPU_PROP_DENSE 1
+#define MSGPU_PREC_BF16X3 2
+#define MSGPU_PREC_BF16X6 3
+
+/* Options (msgpu_set_option). */
+#define MSGPU_OPT_DENSE_RENORMALIZE 1 /* 1 (default): the dense form restores the exact
+                                        Haberkorn survival |psi|^2 e^{-2 kappa t} of each
+                                        trajectory every step (scalar K only); 0: off */
 
 /* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
  * dimensions (the whole time loop in one launch, one warp per trajectory,
@@ -138,13 +152,17 @@ int msgpu_fetch_yields(msgpu_ctx *ctx, double *per_traj, double *ensemble);
 int msgpu_fetch_values(msgpu_ctx *ctx, double *values);
 
 /* Kernel timing with CUDA events on the launch stream.  Classes:
- * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield. */
+ * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield,
+ * 6 dense GEMM (tensor cores). */
 int msgpu_profile_enable(msgpu_ctx *ctx, int enable);
 int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long long *launches);
 
 /* Select the execution form (MSGPU_FORM_*); RESIDENT falls back to an error
  * at run time if the Krylov basis of one trajectory does not fit shared memory. */
 int msgpu_set_form(msgpu_ctx *ctx, int form);
+
+/* Set an option (MSGPU_OPT_*). */
+int msgpu_set_option(msgpu_ctx *ctx, int key, double value);
 
 /* ---------------------------------------------------------------- batching
  * Many spin systems of uneven dimension and trajectory count propagated by

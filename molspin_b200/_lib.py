@@ -29,6 +29,10 @@ REC_AUTO = 0
 REC_ARNOLDI = 1
 REC_LANCZOS = 2
 PROP_KRYLOV = 0
+PROP_DENSE = 1
+PREC_BF16X3 = 2
+PREC_BF16X6 = 3
+OPT_DENSE_RENORMALIZE = 1
 NOISE_NONE = 0
 NOISE_REPLAY = 1
 NOISE_PHILOX = 2
@@ -87,6 +91,7 @@ def _load() -> C.CDLL:
         "msgpu_profile_read": (I, [P, I, pD, C.POINTER(C.c_longlong)]),
         "msgpu_launch_count": (C.c_longlong, [P]),
         "msgpu_set_form": (I, [P, I]),
+        "msgpu_set_option": (I, [P, I, D]),
         "msgpu_batch_create": (P, [I, C.c_size_t]),
         "msgpu_batch_destroy": (None, [P]),
         "msgpu_batch_last_error": (C.c_char_p, [P]),

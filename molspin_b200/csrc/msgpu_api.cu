@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "msgpu_dense.h"
 #include "msgpu_kernels.cuh"
 #include "msgpu_resident.cuh"
 
@@ -19,7 +20,7 @@ using namespace msgpu;
 
 namespace {
 
-enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_N = 6 };
+enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_N = 7 };
 
 struct DevBuf {
     void *p = nullptr;
@@ -49,6 +50,10 @@ struct msgpu_ctx {
     // resident (one warp per trajectory, whole time loop per launch) form
     int form = MSGPU_FORM_AUTO;
     DevBuf colbuf, trajval, times_d, pflip_d, sys_d, work_d, obs_d;
+    // dense tensor-core form
+    msgpu::DenseState dense;
+    std::vector<std::pair<void *, size_t>> dense_allocs;
+    int dense_renorm = 1;
     // reaction
     bool k_scalar = true;
     double kappa = 0.0;
@@ -230,6 +235,7 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
                      &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d};
     for (DevBuf *b : all) release(c, *b);
+    for (auto &a : c->dense_allocs) cudaFree(a.first);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }
@@ -239,6 +245,16 @@ const char *msgpu_last_error(const msgpu_ctx *c) { return c ? c->err.c_str() : "
 size_t msgpu_device_bytes(const msgpu_ctx *c) { return c ? c->used : 0; }
 
 long long msgpu_launch_count(const msgpu_ctx *c) { return c ? c->launches : 0; }
+
+int msgpu_set_option(msgpu_ctx *c, int key, double value)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (key == MSGPU_OPT_DENSE_RENORMALIZE) {
+        c->dense_renorm = value != 0.0;
+        return MSGPU_OK;
+    }
+    return fail(c, MSGPU_ERR_INVALID, "unknown option");
+}
 
 int msgpu_set_form(msgpu_ctx *c, int form)
 {
@@ -529,6 +545,128 @@ int ensure_state(msgpu_ctx *c, int prec)
 }
 
 double flip_p(double st_rate, double h) { return -0.5 * std::expm1(-2.0 * (0.5 * st_rate) * h); }
+
+// Device allocations of the dense form, charged to the context's budget.
+int dense_alloc_cb(void *ctx, void **p, size_t bytes, const char *what)
+{
+    auto *c = static_cast<msgpu_ctx *>(ctx);
+    if (c->budget && c->used + bytes > c->budget)
+        return fail(c, MSGPU_ERR_BUDGET, std::string("device memory budget exceeded allocating ") + what);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(c, e, what);
+    }
+    c->used += bytes;
+    c->dense_allocs.push_back({*p, bytes});
+    return MSGPU_OK;
+}
+
+void dense_release_cb(void *ctx, void *p)
+{
+    auto *c = static_cast<msgpu_ctx *>(ctx);
+    if (!p) return;
+    for (size_t i = 0; i < c->dense_allocs.size(); ++i)
+        if (c->dense_allocs[i].first == p) {
+            cudaFree(p);
+            c->used -= c->dense_allocs[i].second;
+            c->dense_allocs.erase(c->dense_allocs.begin() + i);
+            return;
+        }
+}
+
+int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
+{
+    const int D = c->D, ldm = c->ldm, M = c->M;
+    const int nobs = static_cast<int>(c->obs.size());
+    cudaStream_t st = c->stream;
+    int rc;
+    if ((rc = ensure_state(c, MSGPU_PREC_C128)) ||
+        (rc = ensure(c, c->acc, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield acc")) ||
+        (rc = ensure(c, c->comp, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield comp")) ||
+        (rc = ensure(c, c->prev, static_cast<size_t>(nobs) * ldm * sizeof(double), "yield prev")) ||
+        (rc = ensure(c, c->rates_d, 8 * sizeof(double), "rates")) ||
+        (rc = ensure(c, c->status, sizeof(int), "status")) ||
+        (rc = ensure(c, c->values_d, static_cast<size_t>(p->ntimes) * nobs * sizeof(double), "values")) ||
+        (rc = ensure(c, c->obs_d, 8 * 16 * sizeof(double2), "observables")))
+        return rc;
+    const PairObs po = make_pair_obs(c);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->rates_d.p, c->rates.data(), nobs * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(c->obs_d.p, po.op, sizeof(double2) * 16 * nobs, cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemsetAsync(c->status.p, 0, sizeof(int), st)))
+        return cuda_fail(c, e, "dense setup");
+    if (!p->accumulate) {
+        if ((e = cudaMemsetAsync(c->acc.p, 0, static_cast<size_t>(nobs) * ldm * sizeof(double), st)) ||
+            (e = cudaMemsetAsync(c->comp.p, 0, static_cast<size_t>(nobs) * ldm * sizeof(double), st)))
+            return cuda_fail(c, e, "dense setup");
+    }
+    msgpu::DenseRun run;
+    std::memset(&run, 0, sizeof(run));
+    run.rowptr = static_cast<const int *>(c->hrow.p);
+    run.col = static_cast<const int *>(c->hcol.p);
+    run.val = static_cast<const double *>(c->hval.p);
+    if (!c->k_scalar) {
+        run.krow = static_cast<const int *>(c->krow.p);
+        run.kcol = static_cast<const int *>(c->kcol.p);
+        run.kval = static_cast<const double *>(c->kval.p);
+    }
+    run.kappa = c->k_scalar ? c->kappa : 0.0;
+    run.s1 = c->s1;
+    run.s2 = c->s2;
+    run.nobs = nobs;
+    run.obs = static_cast<const double *>(c->obs_d.p);
+    run.rates = static_cast<const double *>(c->rates_d.p);
+    run.noise_mode = c->noise_mode;
+    run.bits = static_cast<const unsigned char *>(c->bits.p);
+    run.bits_steps = c->bits_steps;
+    run.bits_ntraj = c->bits_ntraj;
+    run.seed = c->seed;
+    run.acc = static_cast<double *>(c->acc.p);
+    run.comp = static_cast<double *>(c->comp.p);
+    run.prev = static_cast<double *>(c->prev.p);
+    run.acc_ld = ldm;
+    run.values = static_cast<double *>(c->values_d.p);
+    run.times = p->times;
+    run.ntimes = p->ntimes;
+    run.step_offset = p->step_offset;
+    run.accumulate = p->accumulate;
+    run.st_rate = c->st_rate;
+    run.renormalize = c->dense_renorm;
+    run.status = static_cast<int *>(c->status.p);
+    const int parts = p->precision == MSGPU_PREC_BF16X6 ? 3 : 2;
+    const double dt = p->ntimes > 1 ? p->times[1] - p->times[0] : 1.0;
+    for (int s = 1; s + 1 < p->ntimes; ++s)
+        if (std::abs((p->times[s + 1] - p->times[s]) - dt) > 1e-12 * std::abs(dt))
+            return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator needs a uniform time step");
+    std::string err;
+    if (c->dense.psi && (c->dense.D != D || c->dense.M != M || c->dense.parts != parts))
+        msgpu::dense_release(c->dense, dense_release_cb, c);  // shape changed: rebuild
+    if ((rc = msgpu::dense_prepare(c->dense, D, M, ldm, parts, dt, run, c->psi128.p, st, err, dense_alloc_cb, c)))
+        return err.empty() ? rc : fail(c, rc, err);
+    float gemm_ms = 0.f;
+    long long gemm_n = 0;
+    c->launches += 3LL * (p->ntimes - 1) + 2;
+    if ((rc = msgpu::dense_run(c->dense, run, c->psi128.p, ldm, st, err, c->prof ? &gemm_ms : nullptr, &gemm_n)))
+        return fail(c, rc, err);
+    if (c->prof) {
+        c->prof_ms[KC_GEMM] += gemm_ms;
+        c->prof_n[KC_GEMM] += gemm_n;
+    }
+    int status = 0;
+    c->last_values.assign(static_cast<size_t>(p->ntimes) * nobs, 0.0);
+    if ((e = cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(c->last_values.data(), c->values_d.p, c->last_values.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+        return cuda_fail(c, e, "dense run");
+    c->state_prec = MSGPU_PREC_C128;
+    c->last_ntimes = p->ntimes;
+    c->have_integrals = true;
+    if (status & 4) return fail(c, MSGPU_ERR_CUDA, "run: dense GEMM pipeline timed out (bounded wait expired)");
+    if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite observable or norm on the device");
+    return MSGPU_OK;
+}
 
 // Warps per CTA of the resident form for this problem, 0 if it does not
 // apply (streamed form forced, dimension too large for the shared-memory
@@ -886,14 +1024,25 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     if (c->s1 == 0) return fail(c, MSGPU_ERR_STATE, "run: electron pair strides not set");
     if (c->D % (2 * c->s1) != 0) return fail(c, MSGPU_ERR_INVALID, "run: electron strides inconsistent with the Hilbert dimension");
     if (c->obs.empty()) return fail(c, MSGPU_ERR_STATE, "run: no observables");
+    for (int s = 0; s < p->ntimes; ++s)
+        if (!std::isfinite(p->times[s]) || (s > 0 && !(p->times[s] > p->times[s - 1])))
+            return fail(c, MSGPU_ERR_INVALID, "run: times must be finite and strictly increasing");
+    if (p->propagator == MSGPU_PROP_DENSE) {
+        if (p->precision != MSGPU_PREC_BF16X3 && p->precision != MSGPU_PREC_BF16X6)
+            return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator takes MSGPU_PREC_BF16X3 or MSGPU_PREC_BF16X6");
+        if (c->D > 4096) return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator is limited to dimension 4096");
+        if (c->noise_mode == MSGPU_NOISE_REPLAY &&
+            (c->bits_ntraj != c->M || p->step_offset < 0 || p->step_offset + (p->ntimes - 1) > c->bits_steps))
+            return fail(c, MSGPU_ERR_INVALID, "run: replay bits do not cover the requested steps");
+        if (p->accumulate && !c->have_integrals) return fail(c, MSGPU_ERR_STATE, "run: nothing to continue (accumulate=1)");
+        if (int rc = device_guard(c)) return rc;
+        return run_dense(c, p);
+    }
     if (p->precision != MSGPU_PREC_C128 && p->precision != MSGPU_PREC_C64)
         return fail(c, MSGPU_ERR_INVALID, "run: unknown precision");
     if (p->propagator != MSGPU_PROP_KRYLOV) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
     if (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov)
         return fail(c, MSGPU_ERR_INVALID, "run: krylov_dim must be in 1..32");
-    for (int s = 0; s < p->ntimes; ++s)
-        if (!std::isfinite(p->times[s]) || (s > 0 && !(p->times[s] > p->times[s - 1])))
-            return fail(c, MSGPU_ERR_INVALID, "run: times must be finite and strictly increasing");
     int rec = p->recurrence;
     if (rec == MSGPU_REC_AUTO) rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
     if (rec == MSGPU_REC_LANCZOS && !c->k_scalar)
@@ -1285,9 +1434,9 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
     int *status = cv.take<int>(1);
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e;
     // Contents left by the previous call are stale: clear what must start at zero.
-    if ((e = cudaMemsetAsync(status, 0, sizeof(int), st)) || (e = cudaMemsetAsync(mdim, 0, ldm * sizeof(int), st)))
+    if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess ||
+        cudaMemsetAsync(mdim, 0, ldm * sizeof(int), st) != cudaSuccess)
         return MSGPU_ERR_CUDA;
     {
         dim3 grid(ceil_div(D, 32), ldm / 32), block(32, 8);
@@ -1326,8 +1475,8 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
     }
     const size_t smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
     const int warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / smem_warp)));
-    if ((e = cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(warps * smem_warp))))
+    if (cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(warps * smem_warp)) != cudaSuccess)
         return MSGPU_ERR_CUDA;
     k_krylov_expm<<<ceil_div(ldm, warps), 32 * warps, warps * smem_warp, st>>>(hess, nullptr, nullptr, 0.0, mdim, beta0,
                                                                               nullptr, m, ldm, ntraj, dt, coef, status);
@@ -1337,10 +1486,10 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
         dim3 g(ceil_div(D, 32), ldm / 32), b(32, 8);
         k_interleaved_to_cols<double2><<<g, b, 0, st>>>(reinterpret_cast<double2 *>(psi_out), psi, D, ntraj, ldm);
     }
-    if ((e = cudaGetLastError())) return MSGPU_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return MSGPU_ERR_CUDA;
     int h_status = 0;
-    if ((e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
-        (e = cudaStreamSynchronize(st)))
+    if (cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
         return MSGPU_ERR_CUDA;
     if (h_status & 2) return MSGPU_ERR_NONFINITE;
     if (h_status & 1) return MSGPU_ERR_EXPM;

@@ -1,0 +1,832 @@
+// msgpu_dense.cu -- dense tensor-core form (MSGPU_PROP_DENSE).
+//
+// For a static H of modest dimension the reference's "normal" propagator
+// (HSPropagator::Step dense branch, HSPropagator.cpp:92-100) applies
+// U = expmat(dt G), G = -iH - K, to the factor block -- rebuilding U every
+// step.  Here U is built once in FP64 on the device (scaling and squaring of
+// a degree-18 Taylor polynomial, Horner form, FP64 complex GEMMs), written as
+// the real 2D x 2D matrix of interleaved (re, im) pairs
+//     A[2r+c][2s+d] = [[Re U, -Im U], [Im U, Re U]]_{rs}[c][d],
+// and split into BF16 parts (x = x_0 + x_1 [+ x_2]).  Each step is then one
+// real GEMM  Psi'^T = A Psi^T  with the trajectory block stored
+// trajectory-major as interleaved complex (the reference's column-major
+// factors), executed on the 5th-generation tensor cores:
+//   * TMA (cp.async.bulk.tensor, 128-byte swizzle) stages A and B tiles in a
+//     two-deep shared-memory ring guarded by mbarriers;
+//   * one thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32
+//     accumulation in TMEM) for every product x_i y_j with i + j < parts;
+//   * the four warps drain TMEM with tcgen05.ld and store Psi' (FP32).
+// A fused epilogue kernel applies the singlet-triplet flips, evaluates the
+// pair observables, advances the trapezoid, optionally restores the exact
+// Haberkorn norm, and re-splits the state for the next step.
+//
+// Every mbarrier wait is bounded: after the limit the kernel records an
+// error, waits (bounded) for its own copies in flight, frees its TMEM and
+// returns.
+
+#include "msgpu_dense.h"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "msgpu.h"
+#include "msgpu_device.cuh"
+
+namespace msgpu {
+namespace {
+
+constexpr int kGM = 128;          // rows of A per CTA (TMEM lanes)
+constexpr int kGK = 64;           // K per stage: 64 BF16 = one 128-byte swizzle row
+constexpr int kGStages = 2;
+constexpr int kGThreads = 128;    // 4 warps
+constexpr int kATile = kGM * kGK * 2;  // bytes of one A part tile (16 KB)
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// The FP32 accumulation of tcgen05.mma rounds towards zero: each MMA
+// shrinks the accumulator by about half an ulp of its own magnitude, so the
+// bias grows with the number of MMAs and with the size of the partial sums.
+// The small split-correction products therefore go to their own accumulator
+// (2^-8 of the main magnitude, so their bias is negligible), and with 3 parts
+// the hi x hi product is spread over 3 K-range accumulators; the epilogue sums
+// the accumulators with round-to-nearest FP32 adds (unbiased).  TMEM: NACC x BN = 512 columns.
+template <int NS>
+struct GemmCfg {
+    static constexpr int BN = NS == 2 ? 256 : 128;       // trajectories per CTA
+    static constexpr int NHI = NS == 2 ? 1 : 3;          // hi x hi accumulators (K ranges)
+    static constexpr int NACC = NHI + 1;                 // + the correction accumulator
+    static constexpr int Cols = NACC * BN;               // TMEM columns (power of two, <= 512)
+    static constexpr int BTile = BN * kGK * 2;           // bytes of one B part tile
+    static constexpr int Stage = NS * kATile + NS * BTile;
+    static constexpr int Smem = kGStages * Stage + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(Cols == 512, "TMEM split");
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; sets *abort (shared) and returns false after the limit or
+// when another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, volatile int *abort)
+{
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        if (mbar_try(addr, parity)) return true;
+        if (*abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :
+        : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major operand, 128-byte swizzle, rows of
+// 128 bytes in 8-row (1024-byte) groups: SBO = 1024 B, LBO unused (1),
+// version 1, layout type SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= static_cast<uint64_t>(2) << 61;
+    return d;
+}
+
+// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+           (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// 32 TMEM lanes x 16 columns (one row per thread); the caller waits with
+// tcgen05.wait::ld before reading v.
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// C^T = sum over products (i, j), i + j < NS, of A_i B_j^T.
+//   A parts: Dp x Dp BF16, row-major (K contiguous)  -> tensor maps ta[0..NS)
+//   B parts: Mp x Dp BF16, row-major (K contiguous)  -> tensor maps tb[0..NS)
+//   out:     Mp x Dp FP32, out[n][m] = C[m][n]
+// grid = (Mp / BN, Dp / 128), block = 128 threads.
+template <int NS>
+__global__ void __launch_bounds__(kGThreads, 1)
+k_dense_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
+             const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
+             const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2, float *__restrict__ out,
+             int Dp, int *__restrict__ status)
+{
+    using Cfg = GemmCfg<NS>;
+    constexpr int BN = Cfg::BN;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned ring (swizzle atoms)
+    unsigned char *base_ptr = smem_raw + (base - raw);
+    const uint32_t bars = base + kGStages * Cfg::Stage;  // full[2], empty[2], accum
+    uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(base_ptr + kGStages * Cfg::Stage);
+    volatile int *abort = reinterpret_cast<volatile int *>(bar_ptr + 8);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ptr + 9);
+    const uint32_t full0 = bars, empty0 = bars + 16, accum = bars + 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kGM;
+    const int nk = Dp / kGK;
+    const CUtensorMap *ta[3] = {&ta0, &ta1, &ta2};
+    const CUtensorMap *tb[3] = {&tb0, &tb1, &tb2};
+
+    if (threadIdx.x == 0) {
+        *abort = 0;
+        for (int s = 0; s < kGStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * s));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * s));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(accum));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(Cfg::Cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kGStages, r = kb / kGStages;
+            if (!mbar_wait(empty0 + 8 * s, (r & 1) ^ 1, abort)) break;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * s),
+                         "r"(Cfg::Stage));
+            const uint32_t st = base + s * Cfg::Stage;
+            for (int p = 0; p < NS; ++p) tma_load_2d(st + p * kATile, ta[p], kb * kGK, m0, full0 + 8 * s);
+            for (int q = 0; q < NS; ++q)
+                tma_load_2d(st + NS * kATile + q * Cfg::BTile, tb[q], kb * kGK, n0, full0 + 8 * s);
+            issued = kb + 1;
+        }
+        // make sure every copy this CTA started has landed before it can exit
+        for (int kb = max(0, issued - kGStages); kb < issued; ++kb) {
+            const int s = kb % kGStages, r = kb / kGStages;
+            for (uint32_t it = 0; it < kWaitLimit && !mbar_try(full0 + 8 * s, r & 1); ++it) {
+            }
+        }
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        constexpr uint32_t idesc = umma_idesc(kGM, BN);
+        const uint32_t corr = tmem + Cfg::NHI * BN;  // correction accumulator
+        uint32_t corr_on = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kGStages, r = kb / kGStages;
+            if (!mbar_wait(full0 + 8 * s, r & 1, abort)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * Cfg::Stage;
+            // hi x hi accumulator of this K range; its first MMA overwrites
+            const int h = kb * Cfg::NHI / nk;
+            const uint32_t hi = tmem + h * BN;
+            const int first_kb = (h * nk + Cfg::NHI - 1) / Cfg::NHI;
+#pragma unroll
+            for (int kk = 0; kk < kGK / 16; ++kk) {
+#pragma unroll
+                for (int p = 0; p < NS; ++p)
+#pragma unroll
+                    for (int q = 0; q < NS; ++q) {
+                        if (p + q >= NS) continue;
+                        const uint64_t ad = umma_desc(st + p * kATile + kk * 32);
+                        const uint64_t bd = umma_desc(st + NS * kATile + q * Cfg::BTile + kk * 32);
+                        if (p + q == 0) {
+                            umma_bf16(hi, ad, bd, idesc, (kb == first_kb && kk == 0) ? 0u : 1u);
+                        } else {
+                            umma_bf16(corr, ad, bd, idesc, corr_on);
+                            corr_on = 1;
+                        }
+                    }
+            }
+            umma_commit(empty0 + 8 * s);
+        }
+        umma_commit(accum);  // tracks completion of every MMA issued above
+    }
+    __syncwarp();
+
+    // epilogue: warp w drains TMEM lanes [32w, 32w+32) = rows m0 + 32w + lane
+    bool ok = mbar_wait(accum, 0, abort);
+    if (!ok) {
+        // still wait (bounded) for the MMAs in flight before TMEM is freed
+        for (uint32_t it = 0; it < kWaitLimit && !mbar_try(accum, 0); ++it) {
+        }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && !*abort) {
+        const int row = m0 + 32 * warp + lane;
+        const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * warp) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            // all accumulators of this column group in flight, one wait
+            uint32_t v[Cfg::NACC][16];
+#pragma unroll
+            for (int a = 0; a < Cfg::NACC; ++a) tmem_ld16_issue(lane_base + static_cast<uint32_t>(a * BN + c), v[a]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                // round-to-nearest FP32 sums: correction first, then the hi
+                // K ranges; a range with no k-block (nk < NHI) was never written
+                float sum = __uint_as_float(v[Cfg::NACC - 1][j]);
+#pragma unroll
+                for (int a = Cfg::NHI - 1; a >= 0; --a)
+                    if ((a * nk + Cfg::NHI - 1) / Cfg::NHI < nk) sum += __uint_as_float(v[a][j]);
+                out[static_cast<size_t>(n0 + c + j) * Dp + row] = sum;
+            }
+        }
+    }
+    if (*abort && threadIdx.x == 0) atomicOr(status, 4);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::Cols));
+    }
+}
+
+// ------------------------------------------------------------ U precompute
+// C = scale * (A B) + (add_identity ? I : 0); n x n complex row-major.
+__global__ void k_zgemm(const double2 *__restrict__ A, const double2 *__restrict__ B, double2 *__restrict__ C, int n,
+                        double scale, int add_identity)
+{
+    __shared__ double2 As[16][17], Bs[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k0 = 0; k0 < n; k0 += 16) {
+        As[ty][tx] = (row < n && k0 + tx < n) ? A[static_cast<size_t>(row) * n + k0 + tx] : make_double2(0.0, 0.0);
+        Bs[ty][tx] = (k0 + ty < n && col < n) ? B[static_cast<size_t>(k0 + ty) * n + col] : make_double2(0.0, 0.0);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc = cfma(As[ty][k], Bs[k][tx], acc);
+        __syncthreads();
+    }
+    if (row < n && col < n) {
+        double2 v = cscale(acc, scale);
+        if (add_identity && row == col) v.x += 1.0;
+        C[static_cast<size_t>(row) * n + col] = v;
+    }
+}
+
+// G = dt * (-iH - K) dense (row-major), from CSR; zero-filled first.
+__global__ void k_dense_generator(const int *__restrict__ rowptr, const int *__restrict__ col,
+                                  const double2 *__restrict__ val, const int *__restrict__ krow,
+                                  const int *__restrict__ kcol, const double2 *__restrict__ kval, double kappa,
+                                  double dt, int n, double2 *__restrict__ G)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+        const double2 h = val[k];
+        G[static_cast<size_t>(r) * n + col[k]] = make_double2(dt * h.y, -dt * h.x);  // -i dt H
+    }
+    if (krow) {
+        for (int k = krow[r]; k < krow[r + 1]; ++k) {
+            double2 &g = G[static_cast<size_t>(r) * n + kcol[k]];
+            g.x -= dt * kval[k].x;
+            g.y -= dt * kval[k].y;
+        }
+    } else {
+        G[static_cast<size_t>(r) * n + r].x -= dt * kappa;
+    }
+}
+
+__global__ void k_row_norms(const double2 *__restrict__ A, int n, double *__restrict__ out)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double s = 0.0;
+    for (int c = 0; c < n; ++c) s += sqrt(cabs2(A[static_cast<size_t>(r) * n + c]));
+    out[r] = s;
+}
+
+// Split an FP64 value into NS BF16 parts (round to nearest at each level).
+__device__ __forceinline__ void split_bf16(double x, int ns, __nv_bfloat16 *p)
+{
+    double r = x;
+    for (int i = 0; i < ns; ++i) {
+        const __nv_bfloat16 h = __double2bfloat16(r);
+        p[i] = h;
+        r -= static_cast<double>(__bfloat162float(h));
+    }
+}
+
+// U (n x n complex) -> real interleaved Dp x Dp matrix, split in parts
+// (parts x Dp x Dp, padding rows/columns zero).
+__global__ void k_u_split(const double2 *__restrict__ U, int n, int Dp, int ns, __nv_bfloat16 *__restrict__ parts)
+{
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<size_t>(Dp) * Dp) return;
+    const int i = static_cast<int>(idx / Dp), j = static_cast<int>(idx % Dp);
+    double x = 0.0;
+    if (i < 2 * n && j < 2 * n) {
+        const double2 u = U[static_cast<size_t>(i >> 1) * n + (j >> 1)];
+        const int c = i & 1, d = j & 1;
+        x = (c == d) ? u.x : (c == 0 ? -u.y : u.y);
+    }
+    __nv_bfloat16 p[3];
+    split_bf16(x, ns, p);
+    for (int k = 0; k < ns; ++k) parts[static_cast<size_t>(k) * Dp * Dp + idx] = p[k];
+}
+
+// context state (ldm x D interleaved complex128) <-> dense state (Mp x Dp fp32)
+__global__ void k_ctx_to_dense(const double2 *__restrict__ psi, int D, int M, int ldm, int Dp, int Mp,
+                               float *__restrict__ out)
+{
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<size_t>(Mp) * Dp) return;
+    const int t = static_cast<int>(idx / Dp), k = static_cast<int>(idx % Dp);
+    float v = 0.f;
+    if (t < M && k < 2 * D) {
+        const double2 z = psi[static_cast<size_t>(k >> 1) * ldm + t];
+        v = static_cast<float>((k & 1) ? z.y : z.x);
+    }
+    out[idx] = v;
+}
+
+__global__ void k_dense_to_ctx(const float *__restrict__ in, int D, int M, int ldm, int Dp, double2 *__restrict__ psi)
+{
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= static_cast<size_t>(D) * ldm) return;
+    const int r = static_cast<int>(idx / ldm), t = static_cast<int>(idx % ldm);
+    double2 z = make_double2(0.0, 0.0);
+    if (t < M) z = make_double2(in[static_cast<size_t>(t) * Dp + 2 * r], in[static_cast<size_t>(t) * Dp + 2 * r + 1]);
+    psi[idx] = z;
+}
+
+struct DenseEpi {
+    int D, Dp, M, Mp, s1, s2, nobs, ns;
+    const double2 *obs;
+    const double *rates;
+    // noise
+    int noise_mode;
+    const unsigned char *bits;
+    long long bits_steps;
+    int bits_ntraj;
+    unsigned long long seed;
+    long long stepA, stepB;
+    int halfA, halfB;
+    double pA, pB;
+    // yields
+    double dt;
+    int init;
+    double *acc, *comp, *prev;
+    int acc_ld;
+    double *tvals;        // M x nobs (this time point)
+    double *norm0;        // per trajectory: |psi(0)|^2 (renormalisation reference)
+    double decay;         // target |psi|^2 = norm0 * exp(-decay * (t - t0))
+    double elapsed;       // t - t0 of this time point
+    int renormalize;
+    int *status;
+};
+
+__device__ __forceinline__ int dense_flip(const DenseEpi &E, int t, long long step, int half, double p)
+{
+    if (step < 0) return 0;
+    if (E.noise_mode == MSGPU_NOISE_REPLAY) {
+        if (t >= E.bits_ntraj || step >= E.bits_steps) return 0;
+        const long long bit = (step * 2 + half) * E.bits_ntraj + t;
+        return (E.bits[bit >> 3] >> (bit & 7)) & 1;
+    }
+    if (E.noise_mode == MSGPU_NOISE_PHILOX)
+        return philox_flip(E.seed, static_cast<uint32_t>(t), static_cast<uint32_t>(step), static_cast<uint32_t>(half),
+                           p) ? 1 : 0;
+    return 0;
+}
+
+// One CTA (128 threads) per trajectory: flips, optional renormalisation,
+// observables, trapezoid, and the BF16 split of the state for the next GEMM.
+__global__ void __launch_bounds__(128) k_dense_epilogue(float *__restrict__ psi, __nv_bfloat16 *__restrict__ bparts,
+                                                        DenseEpi E)
+{
+    __shared__ double red[9][4];
+    __shared__ double s_scale;
+    const int t = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *col = psi + static_cast<size_t>(t) * E.Dp;
+    const int Q = E.D / 4;
+    int flip = 0;
+    if (t < E.M) {
+        flip = dense_flip(E, t, E.stepA, E.halfA, E.pA);
+        if (E.stepB >= 0) flip ^= dense_flip(E, t, E.stepB, E.halfB, E.pB);
+    }
+    // pass 1: flip and norm
+    double nn = 0.0;
+    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+        const int b = quartet_base(q, E.s1, E.s2);
+        const int r[4] = {b, b + E.s2, b + E.s1, b + E.s1 + E.s2};
+        float2 x[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) x[a] = make_float2(col[2 * r[a]], col[2 * r[a] + 1]);
+        if (flip) {
+            const float2 c1 = x[1];
+            x[0] = make_float2(-x[0].x, -x[0].y);
+            x[1] = make_float2(-x[2].x, -x[2].y);
+            x[2] = make_float2(-c1.x, -c1.y);
+            x[3] = make_float2(-x[3].x, -x[3].y);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                col[2 * r[a]] = x[a].x;
+                col[2 * r[a] + 1] = x[a].y;
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) nn += static_cast<double>(x[a].x) * x[a].x + static_cast<double>(x[a].y) * x[a].y;
+    }
+    nn = warp_sum(nn);
+    if (lane == 0) red[8][warp] = nn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double cur = red[8][0] + red[8][1] + red[8][2] + red[8][3];
+        double sc = 1.0;
+        if (E.init) {
+            if (t < E.M) E.norm0[t] = cur;
+        } else if (E.renormalize && cur > 0.0) {
+            sc = sqrt(E.norm0[t] * exp(-E.decay * E.elapsed) / cur);
+        }
+        s_scale = sc;
+    }
+    __syncthreads();
+    const float sc = static_cast<float>(s_scale);
+    // pass 2: scale, observables, split
+    double obs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+        const int b = quartet_base(q, E.s1, E.s2);
+        const int r[4] = {b, b + E.s2, b + E.s1, b + E.s1 + E.s2};
+        double2 v[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float re = col[2 * r[a]] * sc, im = col[2 * r[a] + 1] * sc;
+            if (sc != 1.f) {
+                col[2 * r[a]] = re;
+                col[2 * r[a] + 1] = im;
+            }
+            v[a] = make_double2(re, im);
+        }
+        for (int o = 0; o < E.nobs; ++o) {
+            const double2 *op = E.obs + o * 16;
+            double s = 0.0;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                double2 ox = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) ox = cfma(op[a * 4 + c], v[c], ox);
+                s += v[a].x * ox.x + v[a].y * ox.y;
+            }
+            obs[o] += s;
+        }
+    }
+    __syncthreads();
+    for (int o = 0; o < E.nobs; ++o) {
+        const double w = warp_sum(obs[o]);
+        if (lane == 0) red[o][warp] = w;
+    }
+    // split for the next GEMM (every element of the padded row)
+    for (int k = threadIdx.x; k < E.Dp; k += blockDim.x) {
+        __nv_bfloat16 p[3];
+        split_bf16(static_cast<double>(col[k]), E.ns, p);
+        for (int i = 0; i < E.ns; ++i) bparts[(static_cast<size_t>(i) * E.Mp + t) * E.Dp + k] = p[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && t < E.M) {
+        bool bad = false;
+        for (int o = 0; o < E.nobs; ++o) {
+            const double v = (red[o][0] + red[o][1] + red[o][2] + red[o][3]) * E.rates[o];
+            const size_t k = static_cast<size_t>(o) * E.acc_ld + t;
+            if (!E.init) {
+                const double term = 0.5 * E.dt * (E.prev[k] + v) - E.comp[k];
+                const double s = E.acc[k] + term;
+                E.comp[k] = (s - E.acc[k]) - term;
+                E.acc[k] = s;
+            }
+            E.prev[k] = v;
+            E.tvals[static_cast<size_t>(t) * E.nobs + o] = v;
+            if (!isfinite(v)) bad = true;
+        }
+        if (bad) atomicOr(E.status, 2);
+    }
+}
+
+// values[o] = sum over trajectories of tvals[t][o] (fixed order, one block)
+__global__ void k_dense_values(const double *__restrict__ tvals, int M, int nobs, double *__restrict__ values)
+{
+    __shared__ double red[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = threadIdx.x; t < M; t += blockDim.x)
+        for (int o = 0; o < nobs; ++o) a[o] += tvals[static_cast<size_t>(t) * nobs + o];
+    for (int o = 0; o < nobs; ++o) {
+        const double v = warp_sum(a[o]);
+        if (lane == 0) red[o][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nobs) {
+        double v = 0.0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        values[threadIdx.x] = v;
+    }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder()
+{
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// 2D BF16 tensor map over a rows x cols row-major matrix, box = 64 x box_rows.
+bool make_map(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows)
+{
+    EncodeTiled enc = encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kGK), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+inline int cdiv(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace
+
+int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, const DenseRun &run,
+                  const void *psi128, cudaStream_t stream, std::string &err,
+                  int (*alloc)(void *ctx, void **p, size_t bytes, const char *what), void *actx)
+{
+    if (parts != 2 && parts != 3) { err = "dense: split depth must be 2 or 3"; return MSGPU_ERR_INVALID; }
+    const int BN = parts == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
+    const int Dp = (2 * D + kGM - 1) / kGM * kGM;
+    const int Mp = (M + BN - 1) / BN * BN;
+    const bool realloc = st.D != D || st.M != M || st.parts != parts || !st.psi;
+    if (realloc) {
+        st = DenseState();
+        int rc;
+        if ((rc = alloc(actx, &st.u_parts, sizeof(__nv_bfloat16) * parts * static_cast<size_t>(Dp) * Dp, "dense U")) ||
+            (rc = alloc(actx, &st.psi, sizeof(float) * static_cast<size_t>(Mp) * Dp, "dense state")) ||
+            (rc = alloc(actx, &st.b_parts, sizeof(__nv_bfloat16) * parts * static_cast<size_t>(Mp) * Dp, "dense split state")) ||
+            // G, T, W (+ slack) for U; row norms (8D doubles); per-trajectory
+            // values (8 Mp doubles) and reference norms (Mp doubles)
+            (rc = alloc(actx, &st.work,
+                        sizeof(double2) * 4 * static_cast<size_t>(D) * D +
+                            sizeof(double) * (8 * static_cast<size_t>(D) + 9 * static_cast<size_t>(Mp)),
+                        "dense scratch")))
+            return rc;
+        st.D = D;
+        st.Dp = Dp;
+        st.M = M;
+        st.Mp = Mp;
+        st.parts = parts;
+        st.have_u = false;
+    }
+    cudaError_t e;
+    if (!st.have_u || st.dt != dt) {
+        // U = exp(G) with G = dt(-iH - K): Taylor degree 18 on G / 2^s, then s squarings
+        double2 *G = static_cast<double2 *>(st.work);
+        double2 *T = G + static_cast<size_t>(D) * D, *W = T + static_cast<size_t>(D) * D;
+        double *rn = reinterpret_cast<double *>(W + 2 * static_cast<size_t>(D) * D);
+        cudaMemsetAsync(G, 0, sizeof(double2) * static_cast<size_t>(D) * D, stream);
+        k_dense_generator<<<cdiv(D, 128), 128, 0, stream>>>(run.rowptr, run.col,
+                                                             reinterpret_cast<const double2 *>(run.val), run.krow,
+                                                             run.kcol, reinterpret_cast<const double2 *>(run.kval),
+                                                             run.kappa, dt, D, G);
+        k_row_norms<<<cdiv(D, 128), 128, 0, stream>>>(G, D, rn);
+        std::vector<double> h(D);
+        if ((e = cudaMemcpyAsync(h.data(), rn, sizeof(double) * D, cudaMemcpyDeviceToHost, stream)) ||
+            (e = cudaStreamSynchronize(stream))) {
+            err = std::string("dense: generator: ") + cudaGetErrorString(e);
+            return MSGPU_ERR_CUDA;
+        }
+        double nrm = 0.0;
+        for (double x : h) nrm = std::max(nrm, x);
+        if (!std::isfinite(nrm)) { err = "dense: non-finite generator"; return MSGPU_ERR_NONFINITE; }
+        int s = 0;
+        while (nrm / std::ldexp(1.0, s) > 0.25) ++s;
+        const double inv = std::ldexp(1.0, -s);
+        dim3 gb(cdiv(D, 16), cdiv(D, 16)), tb(16, 16);
+        // Horner: T = I + A/18; T = I + A T / k for k = 17..1
+        cudaMemsetAsync(T, 0, sizeof(double2) * static_cast<size_t>(D) * D, stream);
+        k_zgemm<<<gb, tb, 0, stream>>>(G, T, T, D, 0.0, 1);  // T = I
+        for (int k = 18; k >= 1; --k) {
+            k_zgemm<<<gb, tb, 0, stream>>>(G, T, W, D, inv / k, 1);
+            std::swap(T, W);
+        }
+        for (int q = 0; q < s; ++q) {
+            k_zgemm<<<gb, tb, 0, stream>>>(T, T, W, D, 1.0, 0);
+            std::swap(T, W);
+        }
+        const size_t nu = static_cast<size_t>(Dp) * Dp;
+        k_u_split<<<cdiv(nu, 256), 256, 0, stream>>>(T, D, Dp, parts, static_cast<__nv_bfloat16 *>(st.u_parts));
+        if ((e = cudaGetLastError())) {
+            err = std::string("dense: propagator: ") + cudaGetErrorString(e);
+            return MSGPU_ERR_CUDA;
+        }
+        st.have_u = true;
+        st.dt = dt;
+    }
+    const size_t ns = static_cast<size_t>(Mp) * Dp;
+    k_ctx_to_dense<<<cdiv(ns, 256), 256, 0, stream>>>(static_cast<const double2 *>(psi128), D, M, ldm, Dp, Mp,
+                                                       static_cast<float *>(st.psi));
+    if ((e = cudaGetLastError())) {
+        err = std::string("dense: state: ") + cudaGetErrorString(e);
+        return MSGPU_ERR_CUDA;
+    }
+    return MSGPU_OK;
+}
+
+int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaStream_t stream, std::string &err,
+              float *gemm_ms, long long *gemm_launches)
+{
+    const int D = st.D, Dp = st.Dp, M = st.M, Mp = st.Mp, ns = st.parts;
+    CUtensorMap ta[3], tb[3];
+    std::memset(ta, 0, sizeof(ta));
+    std::memset(tb, 0, sizeof(tb));
+    const int BN = ns == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
+    const __nv_bfloat16 *up = static_cast<const __nv_bfloat16 *>(st.u_parts);
+    __nv_bfloat16 *bp = static_cast<__nv_bfloat16 *>(st.b_parts);
+    for (int p = 0; p < ns; ++p) {
+        if (!make_map(&ta[p], up + static_cast<size_t>(p) * Dp * Dp, Dp, Dp, kGM) ||
+            !make_map(&tb[p], bp + static_cast<size_t>(p) * Mp * Dp, Mp, Dp, BN)) {
+            err = "dense: cannot encode TMA tensor maps (cuTensorMapEncodeTiled unavailable or rejected)";
+            return MSGPU_ERR_CUDA;
+        }
+    }
+    for (int p = ns; p < 3; ++p) {
+        ta[p] = ta[0];
+        tb[p] = tb[0];
+    }
+    cudaError_t e;
+    const int smem = ns == 2 ? GemmCfg<2>::Smem : GemmCfg<3>::Smem;
+    if ((e = cudaFuncSetAttribute(k_dense_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<2>::Smem)) ||
+        (e = cudaFuncSetAttribute(k_dense_gemm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<3>::Smem))) {
+        err = std::string("dense: shared memory: ") + cudaGetErrorString(e);
+        return MSGPU_ERR_CUDA;
+    }
+    double *tvals = reinterpret_cast<double *>(static_cast<double2 *>(st.work) + 4 * static_cast<size_t>(D) * D) + 8 * D;
+    double *norm0 = tvals + 8 * static_cast<size_t>(Mp);
+    DenseEpi E;
+    std::memset(&E, 0, sizeof(E));
+    E.D = D;
+    E.Dp = Dp;
+    E.M = M;
+    E.Mp = Mp;
+    E.s1 = run.s1;
+    E.s2 = run.s2;
+    E.nobs = run.nobs;
+    E.ns = ns;
+    E.obs = reinterpret_cast<const double2 *>(run.obs);
+    E.rates = run.rates;
+    E.noise_mode = run.noise_mode;
+    E.bits = run.bits;
+    E.bits_steps = run.bits_steps;
+    E.bits_ntraj = run.bits_ntraj;
+    E.seed = run.seed;
+    E.acc = run.acc;
+    E.comp = run.comp;
+    E.prev = run.prev;
+    E.acc_ld = run.acc_ld;
+    E.tvals = tvals;
+    E.norm0 = norm0;
+    E.decay = 2.0 * run.kappa;
+    E.renormalize = run.renormalize && run.krow == nullptr;
+    E.status = run.status;
+    const int steps = run.ntimes - 1;
+    auto pstep = [&](int s) {
+        return s < steps ? -0.5 * std::expm1(-2.0 * (0.5 * run.st_rate) * (0.5 * (run.times[s + 1] - run.times[s])))
+                         : 0.0;
+    };
+    // first time point: evaluate, first half-step flip of step 0, split
+    E.stepA = steps > 0 ? run.step_offset : -1;
+    E.halfA = 0;
+    E.pA = pstep(0);
+    E.stepB = -1;
+    E.init = 1;
+    E.dt = 0.0;
+    E.elapsed = 0.0;
+    k_dense_epilogue<<<Mp, 128, 0, stream>>>(static_cast<float *>(st.psi), bp, E);
+    k_dense_values<<<1, 256, 0, stream>>>(tvals, M, run.nobs, run.values);
+    // GEMM launches are bracketed by events only when timing was requested;
+    // the events are read after the loop so the host never waits per step.
+    std::vector<cudaEvent_t> evs;
+    if (gemm_ms) {
+        evs.resize(2 * static_cast<size_t>(steps));
+        for (auto &ev : evs) cudaEventCreate(&ev);
+    }
+    dim3 grid(Mp / BN, Dp / kGM);
+    for (int s = 0; s < steps; ++s) {
+        if (gemm_ms) cudaEventRecord(evs[2 * s], stream);
+        if (ns == 2)
+            k_dense_gemm<2><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
+                                                               static_cast<float *>(st.psi), Dp, run.status);
+        else
+            k_dense_gemm<3><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
+                                                               static_cast<float *>(st.psi), Dp, run.status);
+        if (gemm_ms) cudaEventRecord(evs[2 * s + 1], stream);
+        E.stepA = run.step_offset + s;
+        E.halfA = 1;
+        E.pA = pstep(s);
+        E.stepB = s + 1 < steps ? run.step_offset + s + 1 : -1;
+        E.halfB = 0;
+        E.pB = pstep(s + 1);
+        E.init = 0;
+        E.dt = run.times[s + 1] - run.times[s];
+        E.elapsed = run.times[s + 1] - run.times[0];
+        k_dense_epilogue<<<Mp, 128, 0, stream>>>(static_cast<float *>(st.psi), bp, E);
+        k_dense_values<<<1, 256, 0, stream>>>(tvals, M, run.nobs, run.values + static_cast<size_t>(s + 1) * run.nobs);
+        if ((e = cudaGetLastError())) {
+            err = std::string("dense: step: ") + cudaGetErrorString(e);
+            for (auto &ev : evs) cudaEventDestroy(ev);
+            return MSGPU_ERR_CUDA;
+        }
+    }
+    if (gemm_ms) {
+        float total = 0.f;
+        if (!evs.empty()) cudaEventSynchronize(evs.back());
+        for (int s = 0; s < steps; ++s) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, evs[2 * s], evs[2 * s + 1]);
+            total += ms;
+        }
+        for (auto &ev : evs) cudaEventDestroy(ev);
+        *gemm_ms = total;
+    }
+    if (gemm_launches) *gemm_launches = steps;
+    const size_t nc = static_cast<size_t>(D) * ldm;
+    k_dense_to_ctx<<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const float *>(st.psi), D, M, ldm, Dp,
+                                                       static_cast<double2 *>(psi128));
+    if ((e = cudaGetLastError())) {
+        err = std::string("dense: state: ") + cudaGetErrorString(e);
+        return MSGPU_ERR_CUDA;
+    }
+    return MSGPU_OK;
+}
+
+void dense_release(DenseState &st, void (*release)(void *ctx, void *p), void *ctx)
+{
+    release(ctx, st.u_parts);
+    release(ctx, st.psi);
+    release(ctx, st.b_parts);
+    release(ctx, st.work);
+    st = DenseState();
+}
+
+}  // namespace msgpu

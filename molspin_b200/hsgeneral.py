@@ -151,11 +151,15 @@ class HSPropagatorB200:
         return out.T
 
     # ------------------------------------------------------------ propagation
+    PRECISIONS = {"c128": L.PREC_C128, "c64": L.PREC_C64, "bf16x3": L.PREC_BF16X3, "bf16x6": L.PREC_BF16X6}
+
     def propagate(self, times: np.ndarray, krylov: int, precision: str = "c128", step_offset: int = 0,
-                  accumulate: bool = False, recurrence: int = L.REC_AUTO):
+                  accumulate: bool = False, recurrence: int = L.REC_AUTO, propagator: str = "krylov"):
+        """propagator "krylov" (precision c128 | c64) or "dense" (bf16x3 | bf16x6, tensor cores)."""
         t = np.ascontiguousarray(times, dtype=np.float64)
-        p = L.RunParams(L.dptr(t), len(t), int(krylov), L.PREC_C128 if precision == "c128" else L.PREC_C64,
-                        int(recurrence), L.PROP_KRYLOV, int(step_offset), 1 if accumulate else 0)
+        prop = L.PROP_DENSE if propagator == "dense" else L.PROP_KRYLOV
+        p = L.RunParams(L.dptr(t), len(t), int(krylov), self.PRECISIONS[precision], int(recurrence), prop,
+                        int(step_offset), 1 if accumulate else 0)
         _check(self.ctx, L.lib.msgpu_run(self.ctx, C.byref(p)))
         self._last_ntimes = len(t)
 
@@ -169,6 +173,9 @@ class HSPropagatorB200:
         v = np.zeros((self._last_ntimes, self.nobs), dtype=np.float64)
         _check(self.ctx, L.lib.msgpu_fetch_values(self.ctx, L.dptr(v)))
         return v
+
+    def set_option(self, key: int, value: float):
+        _check(self.ctx, L.lib.msgpu_set_option(self.ctx, int(key), float(value)))
 
     def set_form(self, form: str | int):
         """"auto" | "streamed" | "resident" (see MSGPU_FORM_* in include/msgpu.h)."""
