@@ -616,6 +616,7 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
     run.s2 = c->s2;
     run.nobs = nobs;
     run.obs = static_cast<const double *>(c->obs_d.p);
+    run.obs_host = reinterpret_cast<const double *>(po.op);
     run.rates = static_cast<const double *>(c->rates_d.p);
     run.noise_mode = c->noise_mode;
     run.bits = static_cast<const unsigned char *>(c->bits.p);
@@ -646,7 +647,7 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
         return err.empty() ? rc : fail(c, rc, err);
     float gemm_ms = 0.f;
     long long gemm_n = 0;
-    c->launches += 3LL * (p->ntimes - 1) + 2;
+    c->launches += 2LL * (p->ntimes - 1) + 4;  // GEMM + epilogue per step; first epilogue, last values, two layout copies
     if ((rc = msgpu::dense_run(c->dense, run, c->psi128.p, ldm, st, err, c->prof ? &gemm_ms : nullptr, &gemm_n)))
         return fail(c, rc, err);
     if (c->prof) {

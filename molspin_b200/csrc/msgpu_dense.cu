@@ -404,7 +404,11 @@ __global__ void k_dense_to_ctx(const float *__restrict__ in, int D, int M, int l
 
 struct DenseEpi {
     int D, Dp, M, Mp, s1, s2, nobs, ns;
-    const double2 *obs;
+    // pair observable o as upper-triangle coefficients over the quartet's
+    // (a <= c) pairs: Re <x|O|x> = sum Cr P_ac - Ci Q_ac with P = Re(x_a* x_c),
+    // Q = Im(x_a* x_c), C_ac = O_ac + conj(O_ca) (a < c), C_aa = Re O_aa
+    double2 obs_c[8][10];
+    unsigned obs_mask[8];  // bit k: obs_c[o][k] != 0 (most pair operators are sparse)
     const double *rates;
     // noise
     int noise_mode;
@@ -425,6 +429,9 @@ struct DenseEpi {
     double decay;         // target |psi|^2 = norm0 * exp(-decay * (t - t0))
     double elapsed;       // t - t0 of this time point
     int renormalize;
+    int store_state;            // write the FP32 state back (last time point of a run)
+    const double *prev_tvals;   // previous time point's per-trajectory values, or null
+    double *prev_values;        // its ensemble values (nobs doubles)
     int *status;
 };
 
@@ -442,29 +449,74 @@ __device__ __forceinline__ int dense_flip(const DenseEpi &E, int t, long long st
     return 0;
 }
 
-// One CTA (128 threads) per trajectory: flips, optional renormalisation,
-// observables, trapezoid, and the BF16 split of the state for the next GEMM.
-__global__ void __launch_bounds__(128) k_dense_epilogue(float *__restrict__ psi, __nv_bfloat16 *__restrict__ bparts,
-                                                        DenseEpi E)
+// Ensemble value of one observable: the sum over trajectories of tvals[t][o]
+// in a fixed order (256 threads, strided partial sums, warp tree, warp order).
+__device__ __forceinline__ double dense_ensemble_sum(const double *__restrict__ tvals, int M, int nobs, int o,
+                                                    double (*red)[8])
 {
-    __shared__ double red[9][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double a = 0.0;
+    for (int t = threadIdx.x; t < M; t += blockDim.x) a += tvals[static_cast<size_t>(t) * nobs + o];
+    a = warp_sum(a);
+    if (lane == 0) red[0][warp] = a;
+    __syncthreads();
+    double v = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) v += red[0][w];
+    return v;
+}
+
+// One CTA (256 threads) per trajectory.  The trajectory's column (2D floats,
+// re/im per row) is staged in shared memory once; flips, the norm, the
+// optional renormalisation, the pair observables and the BF16 split of the
+// next GEMM operand all work from there, and the FP32 column is written back
+// only at the last time point (the next GEMM overwrites it otherwise).
+// Blocks 0..nobs-1 also sum the previous time point's per-trajectory values
+// into its ensemble values, which saves a launch per step.
+constexpr int kEpiThreads = 128;
+__global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__restrict__ psi,
+                                                                __nv_bfloat16 *__restrict__ bparts, DenseEpi E)
+{
+    extern __shared__ float4 s_col4[];  // D/2 float4 = the 2D floats of the column
+    float2 *s_col = reinterpret_cast<float2 *>(s_col4);
+    __shared__ double red[9][8];
     __shared__ double s_scale;
+    __shared__ double2 s_obs[8][10];
     const int t = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *col = psi + static_cast<size_t>(t) * E.Dp;
+    if (threadIdx.x < 80) s_obs[threadIdx.x / 10][threadIdx.x % 10] = E.obs_c[threadIdx.x / 10][threadIdx.x % 10];
+    const int n4 = E.D / 2;
+    for (int i = threadIdx.x; i < n4; i += kEpiThreads) s_col4[i] = reinterpret_cast<const float4 *>(col)[i];
     const int Q = E.D / 4;
     int flip = 0;
     if (t < E.M) {
         flip = dense_flip(E, t, E.stepA, E.halfA, E.pA);
         if (E.stepB >= 0) flip ^= dense_flip(E, t, E.stepB, E.halfB, E.pB);
     }
-    // pass 1: flip and norm
+    // the scalars of this trajectory, fetched while the column loads: the
+    // renormalisation reference (thread 0) and, for thread o < nobs, the
+    // trapezoid state of observable o
+    const bool yield_thread = t < E.M && static_cast<int>(threadIdx.x) < E.nobs;
+    const size_t yk = static_cast<size_t>(threadIdx.x) * E.acc_ld + t;
+    double y_prev = 0.0, y_acc = 0.0, y_comp = 0.0;
+    if (yield_thread && !E.init) {
+        y_prev = E.prev[yk];
+        y_acc = E.acc[yk];
+        y_comp = E.comp[yk];
+    }
+    const double ref = (threadIdx.x == 0 && t < E.M && !E.init) ? E.norm0[t] : 0.0;
+    __syncthreads();
+    // one pass over the quartets (each belongs to one thread): flip in shared
+    // memory, norm and pair observables of the unscaled state.  Observables
+    // are quadratic, so the renormalisation enters as sc^2 afterwards.
     double nn = 0.0;
-    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+    double obs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int q = threadIdx.x; q < Q; q += kEpiThreads) {
         const int b = quartet_base(q, E.s1, E.s2);
         const int r[4] = {b, b + E.s2, b + E.s1, b + E.s1 + E.s2};
         float2 x[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) x[a] = make_float2(col[2 * r[a]], col[2 * r[a] + 1]);
+        for (int a = 0; a < 4; ++a) x[a] = s_col[r[a]];
         if (flip) {
             const float2 c1 = x[1];
             x[0] = make_float2(-x[0].x, -x[0].y);
@@ -472,106 +524,119 @@ __global__ void __launch_bounds__(128) k_dense_epilogue(float *__restrict__ psi,
             x[2] = make_float2(-c1.x, -c1.y);
             x[3] = make_float2(-x[3].x, -x[3].y);
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                col[2 * r[a]] = x[a].x;
-                col[2 * r[a] + 1] = x[a].y;
-            }
+            for (int a = 0; a < 4; ++a) s_col[r[a]] = x[a];
         }
+        double2 v[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) nn += static_cast<double>(x[a].x) * x[a].x + static_cast<double>(x[a].y) * x[a].y;
+        for (int a = 0; a < 4; ++a) v[a] = make_double2(x[a].x, x[a].y);
+        nn += v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y + v[2].x * v[2].x +
+              v[2].y * v[2].y + v[3].x * v[3].x + v[3].y * v[3].y;
+        const volatile double2 *so = &s_obs[0][0];  // re-read per use: nothing is held in registers
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            if (o >= E.nobs) break;
+            const unsigned m = E.obs_mask[o];
+            double sum = 0.0;
+            int k = 0;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = a; c < 4; ++c, ++k)
+                    if ((m >> k) & 1u) {
+                        const double cr = so[o * 10 + k].x, ci = so[o * 10 + k].y;
+                        sum += cr * (v[a].x * v[c].x + v[a].y * v[c].y) - ci * (v[a].x * v[c].y - v[a].y * v[c].x);
+                    }
+            obs[o] += sum;
+        }
     }
     nn = warp_sum(nn);
     if (lane == 0) red[8][warp] = nn;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        if (o >= E.nobs) break;
+        const double w = warp_sum(obs[o]);
+        if (lane == 0) red[o][warp] = w;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const double cur = red[8][0] + red[8][1] + red[8][2] + red[8][3];
+        double cur = 0.0;
+        for (int w = 0; w < kEpiThreads / 32; ++w) cur += red[8][w];
         double sc = 1.0;
         if (E.init) {
             if (t < E.M) E.norm0[t] = cur;
         } else if (E.renormalize && cur > 0.0) {
-            sc = sqrt(E.norm0[t] * exp(-E.decay * E.elapsed) / cur);
+            sc = sqrt(ref * exp(-E.decay * E.elapsed) / cur);
         }
         s_scale = sc;
     }
     __syncthreads();
-    const float sc = static_cast<float>(s_scale);
-    // pass 2: scale, observables, split
-    double obs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
-        const int b = quartet_base(q, E.s1, E.s2);
-        const int r[4] = {b, b + E.s2, b + E.s1, b + E.s1 + E.s2};
-        double2 v[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const float re = col[2 * r[a]] * sc, im = col[2 * r[a] + 1] * sc;
+    const double scd = s_scale;
+    const float sc = static_cast<float>(scd);
+    // BF16 split of the scaled state for the next GEMM: 8 floats (two float4)
+    // per thread and part, 16-byte stores, the padding beyond 2D floats zero.
+    // In FP32 each residual x - bf16(x) is exact, so hi + mid + lo carries all
+    // 24 bits of x; conversions are round-to-nearest, two values at a time.
+    const int nc = E.Dp / 8, live = E.D / 4;  // chunks of 8 floats; 2D / 8 of them hold data
+    float4 *col4 = reinterpret_cast<float4 *>(col);
+    for (int c = threadIdx.x; c < nc; c += kEpiThreads) {
+        float f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (c < live) {
+            float4 u = s_col4[2 * c], w = s_col4[2 * c + 1];
             if (sc != 1.f) {
-                col[2 * r[a]] = re;
-                col[2 * r[a] + 1] = im;
+                u = make_float4(u.x * sc, u.y * sc, u.z * sc, u.w * sc);
+                w = make_float4(w.x * sc, w.y * sc, w.z * sc, w.w * sc);
             }
-            v[a] = make_double2(re, im);
+            if (E.store_state) {
+                col4[2 * c] = u;
+                col4[2 * c + 1] = w;
+            }
+            f[0] = u.x; f[1] = u.y; f[2] = u.z; f[3] = u.w;
+            f[4] = w.x; f[5] = w.y; f[6] = w.z; f[7] = w.w;
         }
-        for (int o = 0; o < E.nobs; ++o) {
-            const double2 *op = E.obs + o * 16;
-            double s = 0.0;
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                double2 ox = make_double2(0.0, 0.0);
+        for (int i = 0; i < 3; ++i) {
+            if (i >= E.ns) break;
+            __align__(16) __nv_bfloat162 h[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) ox = cfma(op[a * 4 + c], v[c], ox);
-                s += v[a].x * ox.x + v[a].y * ox.y;
+            for (int j = 0; j < 4; ++j) {
+                h[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                f[2 * j] -= __low2float(h[j]);
+                f[2 * j + 1] -= __high2float(h[j]);
             }
-            obs[o] += s;
+            *reinterpret_cast<uint4 *>(bparts + (static_cast<size_t>(i) * E.Mp + t) * E.Dp + 8 * c) =
+                *reinterpret_cast<const uint4 *>(h);
         }
     }
-    __syncthreads();
-    for (int o = 0; o < E.nobs; ++o) {
-        const double w = warp_sum(obs[o]);
-        if (lane == 0) red[o][warp] = w;
-    }
-    // split for the next GEMM (every element of the padded row)
-    for (int k = threadIdx.x; k < E.Dp; k += blockDim.x) {
-        __nv_bfloat16 p[3];
-        split_bf16(static_cast<double>(col[k]), E.ns, p);
-        for (int i = 0; i < E.ns; ++i) bparts[(static_cast<size_t>(i) * E.Mp + t) * E.Dp + k] = p[i];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && t < E.M) {
-        bool bad = false;
-        for (int o = 0; o < E.nobs; ++o) {
-            const double v = (red[o][0] + red[o][1] + red[o][2] + red[o][3]) * E.rates[o];
-            const size_t k = static_cast<size_t>(o) * E.acc_ld + t;
-            if (!E.init) {
-                const double term = 0.5 * E.dt * (E.prev[k] + v) - E.comp[k];
-                const double s = E.acc[k] + term;
-                E.comp[k] = (s - E.acc[k]) - term;
-                E.acc[k] = s;
-            }
-            E.prev[k] = v;
-            E.tvals[static_cast<size_t>(t) * E.nobs + o] = v;
-            if (!isfinite(v)) bad = true;
+    // trapezoid (compensated) and this time point's value, one thread per observable
+    if (yield_thread) {
+        const int o = threadIdx.x;
+        double vs = 0.0;
+        for (int w = 0; w < kEpiThreads / 32; ++w) vs += red[o][w];
+        const double v = vs * scd * scd * E.rates[o];
+        if (!E.init) {
+            const double term = 0.5 * E.dt * (y_prev + v) - y_comp;
+            const double s = y_acc + term;
+            E.comp[yk] = (s - y_acc) - term;
+            E.acc[yk] = s;
         }
-        if (bad) atomicOr(E.status, 2);
+        E.prev[yk] = v;
+        E.tvals[static_cast<size_t>(t) * E.nobs + o] = v;
+        if (!isfinite(v)) atomicOr(E.status, 2);
+    }
+    if (E.prev_tvals && blockIdx.x < E.nobs) {
+        __syncthreads();  // red[0] is reused below
+        const double v = dense_ensemble_sum(E.prev_tvals, E.M, E.nobs, blockIdx.x, red);
+        if (threadIdx.x == 0) E.prev_values[blockIdx.x] = v;
     }
 }
 
-// values[o] = sum over trajectories of tvals[t][o] (fixed order, one block)
-__global__ void k_dense_values(const double *__restrict__ tvals, int M, int nobs, double *__restrict__ values)
+// values[o] = ensemble value of the last time point (same order as above)
+__global__ void __launch_bounds__(kEpiThreads) k_dense_values(const double *__restrict__ tvals, int M, int nobs,
+                                                              double *__restrict__ values)
 {
-    __shared__ double red[8][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = threadIdx.x; t < M; t += blockDim.x)
-        for (int o = 0; o < nobs; ++o) a[o] += tvals[static_cast<size_t>(t) * nobs + o];
-    for (int o = 0; o < nobs; ++o) {
-        const double v = warp_sum(a[o]);
-        if (lane == 0) red[o][warp] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < nobs) {
-        double v = 0.0;
-        for (int w = 0; w < (blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
-        values[threadIdx.x] = v;
-    }
+    __shared__ double red[9][8];
+    const double v = dense_ensemble_sum(tvals, M, nobs, blockIdx.x, red);
+    if (threadIdx.x == 0) values[blockIdx.x] = v;
 }
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -628,7 +693,7 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
             // values (8 Mp doubles) and reference norms (Mp doubles)
             (rc = alloc(actx, &st.work,
                         sizeof(double2) * 4 * static_cast<size_t>(D) * D +
-                            sizeof(double) * (8 * static_cast<size_t>(D) + 9 * static_cast<size_t>(Mp)),
+                            sizeof(double) * (8 * static_cast<size_t>(D) + 17 * static_cast<size_t>(Mp)),
                         "dense scratch")))
             return rc;
         st.D = D;
@@ -722,7 +787,11 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         return MSGPU_ERR_CUDA;
     }
     double *tvals = reinterpret_cast<double *>(static_cast<double2 *>(st.work) + 4 * static_cast<size_t>(D) * D) + 8 * D;
-    double *norm0 = tvals + 8 * static_cast<size_t>(Mp);
+    // per-trajectory values of the current and the previous time point
+    // (8 observables at most each), then the renormalisation references
+    double *tv[2] = {tvals, tvals + 8 * static_cast<size_t>(Mp)};
+    double *norm0 = tvals + 16 * static_cast<size_t>(Mp);
+    const size_t epi_smem = sizeof(float) * 2 * static_cast<size_t>(D);
     DenseEpi E;
     std::memset(&E, 0, sizeof(E));
     E.D = D;
@@ -733,7 +802,17 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     E.s2 = run.s2;
     E.nobs = run.nobs;
     E.ns = ns;
-    E.obs = reinterpret_cast<const double2 *>(run.obs);
+    for (int o = 0; o < run.nobs && o < 8; ++o) {
+        const double *op = run.obs_host + 32 * o;  // 16 complex, row-major
+        int k = 0;
+        for (int a = 0; a < 4; ++a)
+            for (int c = a; c < 4; ++c, ++k) {
+                const double re_ac = op[2 * (4 * a + c)], im_ac = op[2 * (4 * a + c) + 1];
+                const double re_ca = op[2 * (4 * c + a)], im_ca = op[2 * (4 * c + a) + 1];
+                E.obs_c[o][k] = a == c ? make_double2(re_ac, 0.0) : make_double2(re_ac + re_ca, im_ac - im_ca);
+                if (E.obs_c[o][k].x != 0.0 || E.obs_c[o][k].y != 0.0) E.obs_mask[o] |= 1u << k;
+            }
+    }
     E.rates = run.rates;
     E.noise_mode = run.noise_mode;
     E.bits = run.bits;
@@ -744,7 +823,7 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     E.comp = run.comp;
     E.prev = run.prev;
     E.acc_ld = run.acc_ld;
-    E.tvals = tvals;
+    E.tvals = tv[0];
     E.norm0 = norm0;
     E.decay = 2.0 * run.kappa;
     E.renormalize = run.renormalize && run.krow == nullptr;
@@ -762,8 +841,10 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     E.init = 1;
     E.dt = 0.0;
     E.elapsed = 0.0;
-    k_dense_epilogue<<<Mp, 128, 0, stream>>>(static_cast<float *>(st.psi), bp, E);
-    k_dense_values<<<1, 256, 0, stream>>>(tvals, M, run.nobs, run.values);
+    E.store_state = steps == 0;
+    E.prev_tvals = nullptr;
+    E.prev_values = nullptr;
+    k_dense_epilogue<<<Mp, kEpiThreads, epi_smem, stream>>>(static_cast<float *>(st.psi), bp, E);
     // GEMM launches are bracketed by events only when timing was requested;
     // the events are read after the loop so the host never waits per step.
     std::vector<cudaEvent_t> evs;
@@ -790,8 +871,11 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         E.init = 0;
         E.dt = run.times[s + 1] - run.times[s];
         E.elapsed = run.times[s + 1] - run.times[0];
-        k_dense_epilogue<<<Mp, 128, 0, stream>>>(static_cast<float *>(st.psi), bp, E);
-        k_dense_values<<<1, 256, 0, stream>>>(tvals, M, run.nobs, run.values + static_cast<size_t>(s + 1) * run.nobs);
+        E.tvals = tv[(s + 1) & 1];
+        E.prev_tvals = tv[s & 1];  // time point s, summed by blocks 0..nobs-1
+        E.prev_values = run.values + static_cast<size_t>(s) * run.nobs;
+        E.store_state = s + 1 == steps;
+        k_dense_epilogue<<<Mp, kEpiThreads, epi_smem, stream>>>(static_cast<float *>(st.psi), bp, E);
         if ((e = cudaGetLastError())) {
             err = std::string("dense: step: ") + cudaGetErrorString(e);
             for (auto &ev : evs) cudaEventDestroy(ev);
@@ -810,6 +894,9 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         *gemm_ms = total;
     }
     if (gemm_launches) *gemm_launches = steps;
+    // ensemble values of the last time point
+    k_dense_values<<<run.nobs, kEpiThreads, 0, stream>>>(tv[steps & 1], M, run.nobs,
+                                                         run.values + static_cast<size_t>(steps) * run.nobs);
     const size_t nc = static_cast<size_t>(D) * ldm;
     k_dense_to_ctx<<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const float *>(st.psi), D, M, ldm, Dp,
                                                        static_cast<double2 *>(psi128));

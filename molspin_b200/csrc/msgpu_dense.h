@@ -34,6 +34,7 @@ struct DenseRun {
     int s1, s2;               // electron strides
     int nobs;
     const double *obs;        // device: nobs x 16 complex (kernel pair basis)
+    const double *obs_host;   // host copy of the same operators
     const double *rates;      // device: nobs
     int noise_mode;
     const unsigned char *bits;

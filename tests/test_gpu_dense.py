@@ -114,6 +114,36 @@ def test_dense_d1024_against_complex128_krylov(precision, tol_traj, tol_ens):
     assert _rel(values, val128) < tol_traj
 
 
+def test_dense_chunked_run_matches_one_run():
+    # a run split into chunks (step_offset + accumulate) continues the noise
+    # stream, the trapezoid and the per-time-point values of one long run
+    system = h.random_system([2, 3], [2, 2], seed=12, st_rate=0.08, hf_scale=3.0)
+    M, times = 70, S.time_grid(60.0, 1.0)
+    F = system.trace_samples(M, 3.0)
+    noise = (system.st_rate, L.NOISE_PHILOX, 4242)
+    with hs.HSPropagatorB200(0) as p:
+        p.set_hamiltonian(*system.hamiltonian_csr())
+        p.set_reaction(kappa=system.kappa())
+        p.set_electron_pair(*system.electron_strides())
+        p.set_observables([(op, rate) for _, op, rate in system.observables()])
+        p.set_noise(*noise)
+        p.set_factors(F)
+        p.propagate(times, 16, "bf16x6", propagator="dense")
+        per1, ens1 = p.yields()
+        val1 = p.values()
+        p.set_factors(F)
+        vals, start = [], 0
+        for k, stop in enumerate([17, 33, 60]):
+            p.propagate(times[start:stop + 1], 16, "bf16x6", step_offset=start, accumulate=k > 0, propagator="dense")
+            vals.append(p.values() if k == 0 else p.values()[1:])
+            start = stop
+        per2, ens2 = p.yields()
+        val2 = np.concatenate(vals)
+    assert _rel(per2, per1) < 1e-6
+    assert _rel(ens2, ens1) < 1e-6
+    assert _rel(val2, val1) < 1e-6
+
+
 def test_dense_error_paths():
     w = S.plain_small()
     F = w.system.trace_samples(8, w.seed)
