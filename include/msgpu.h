@@ -174,7 +174,11 @@ int msgpu_set_option(msgpu_ctx *ctx, int key, double value);
  * K = kappa I, Philox noise keyed by (seed, trajectory, step, half).
  * Systems with dimension >= the team threshold get a whole CTA per
  * trajectory, smaller ones a warp; msgpu_batch_tune picks the threshold and
- * the persistent grid size by timing the batch itself. */
+ * the persistent grid size by timing the batch itself.  Systems of dimension
+ * >= 2048 instead run the streamed single-system path (all trajectories in
+ * lockstep through the quartet-block SpMM) on their own context and stream,
+ * concurrently with the persistent launch; msgpu_batch_run returns when all
+ * are done and its stats report the wall time of the whole run. */
 typedef struct msgpu_batch msgpu_batch;
 msgpu_batch *msgpu_batch_create(int device, size_t hbm_budget_bytes);
 void msgpu_batch_destroy(msgpu_batch *batch);
@@ -190,6 +194,9 @@ int msgpu_batch_run(msgpu_batch *batch, const double *times, int ntimes, int kry
                     int accumulate);
 int msgpu_batch_fetch_yields(msgpu_batch *batch, int system, double *per_traj, double *ensemble);
 int msgpu_batch_stats(const msgpu_batch *batch, double *last_run_ms, int *team_threshold, int *ctas_per_sm);
+/* Kernels launched by the batch since creation (graph replays of the
+ * persistent launch count once each), streamed systems included. */
+long long msgpu_batch_launch_count(const msgpu_batch *batch);
 
 /* Number of kernels this context launched since creation. */
 long long msgpu_launch_count(const msgpu_ctx *ctx);

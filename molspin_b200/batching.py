@@ -83,6 +83,9 @@ class BatchB200:
         self._check(L.lib.msgpu_batch_fetch_yields(self.b, int(index), L.dptr(per), L.dptr(ens)))
         return per, ens
 
+    def launch_count(self) -> int:
+        return int(L.lib.msgpu_batch_launch_count(self.b))
+
     def stats(self):
         ms = C.c_double(0.0)
         th = C.c_int(0)

@@ -1,16 +1,24 @@
 // msgpu_batch.cu -- C ABI of the batching form (include/msgpu.h,
 // msgpu_batch_*): many radical-pair systems of uneven dimension and
-// trajectory count propagated together by one persistent launch
-// (k_batch), replayed from a CUDA graph, with the team threshold and the
-// persistent grid size picked by an autotuner on the batch itself.
+// trajectory count propagated together.  Systems below kStreamDim run in
+// one persistent launch (k_batch), replayed from a CUDA graph, with the team
+// threshold and the persistent grid size picked by an autotuner on the batch
+// itself.  A large system is better served by the streamed single-system
+// path, which advances all its trajectories in lockstep through the
+// quartet-block SpMM (one read of H per 64 trajectories instead of one per
+// trajectory): those systems get their own context and stream and run
+// concurrently with the persistent launch and with each other.
 
 #include "msgpu.h"
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "msgpu_batch.cuh"
@@ -24,11 +32,18 @@ struct Buf {
     size_t bytes = 0;
 };
 
+// Systems of at least this dimension take the streamed single-system path
+// (measured on the 64-system benchmark batch: the persistent teams win below
+// it, the lockstep SpMM above it).
+constexpr int kStreamDim = 2048;
+constexpr int kStreamWorkers = 8;  // host threads driving streamed systems
+
 struct BatchSystem {
     int D = 0, M = 0, nobs = 0, s1 = 0, s2 = 0;
     double kappa = 0.0, st_rate = 0.0;
     unsigned long long seed = 0;
     Buf rowptr, col, valf, obs, rates, psi, acc, comp, prev, pflip;
+    msgpu_ctx *ctx = nullptr;  // streamed single-system path (D >= kStreamDim)
 };
 
 }  // namespace
@@ -46,6 +61,7 @@ struct msgpu_batch {
     size_t graph_key = 0;
     float last_ms = 0.f;
     int m = 0;
+    long long launches = 0;  // persistent launches (tuning probes included)
 };
 
 namespace {
@@ -139,6 +155,7 @@ int prepare(msgpu_batch *b, int ntimes, int m, int accumulate, long long step_of
         S.step_offset = step_offset;
         S.accumulate = accumulate;
         desc[i] = S;
+        if (s.ctx) continue;  // streamed path: no work items here
         auto &dst = s.D >= threshold ? large : small;
         for (int t = 0; t < s.M; ++t) dst.push_back(ResidentWork{static_cast<int>(i), t});
         if (s.D >= threshold) dmax_large = std::max(dmax_large, s.D);
@@ -217,6 +234,7 @@ int set_times(msgpu_batch *b, const double *times, int ntimes)
     if (int rc = upload(b, b->times_d, times, sizeof(double) * ntimes, "times")) return rc;
     std::vector<double> pf(ntimes, 0.0);
     for (auto &s : b->sys) {
+        if (s.ctx) continue;
         for (int k = 0; k + 1 < ntimes; ++k) pf[k] = flip_prob(s.st_rate, 0.5 * (times[k + 1] - times[k]));
         if (int rc = upload(b, s.pflip, pf.data(), sizeof(double) * ntimes, "flip probabilities")) return rc;
     }
@@ -224,18 +242,48 @@ int set_times(msgpu_batch *b, const double *times, int ntimes)
 }
 
 int run_once(msgpu_batch *b, int ntimes, int m, int accumulate, long long step_offset, int threshold, int cps,
-             bool graph, float *ms)
+             bool graph, float *ms, const double *times = nullptr)
 {
     int grid, nlarge, nitems;
     size_t slice, smem;
     if (int rc = prepare(b, ntimes, m, accumulate, step_offset, threshold, cps, &grid, &slice, &smem, &nlarge, &nitems))
         return rc;
+    const auto w0 = std::chrono::steady_clock::now();
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, b->stream);
-    int rc = launch(b, grid, slice, smem, nlarge, nitems, m, graph);
+    int rc = nitems > 0 ? launch(b, grid, slice, smem, nlarge, nitems, m, graph) : MSGPU_OK;
+    if (nitems > 0) b->launches += graph ? 1 : 3;  // a replay of the captured graph, or memsets + kernel
     cudaEventRecord(e1, b->stream);
+    // streamed systems (times given: a real run, not a tuning probe), each on
+    // its own context and stream, while the persistent launch runs
+    std::vector<int> routed;
+    if (times)
+        for (size_t i = 0; i < b->sys.size(); ++i)
+            if (b->sys[i].ctx) routed.push_back(static_cast<int>(i));
+    std::vector<int> rcs(routed.size(), MSGPU_OK);
+    if (!routed.empty() && rc == MSGPU_OK) {
+        msgpu_run_params p;
+        std::memset(&p, 0, sizeof(p));
+        p.times = times;
+        p.ntimes = ntimes;
+        p.krylov_dim = m;
+        p.precision = MSGPU_PREC_C64;
+        p.recurrence = MSGPU_REC_AUTO;
+        p.propagator = MSGPU_PROP_KRYLOV;
+        p.step_offset = step_offset;
+        p.accumulate = accumulate;
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t k; (k = next.fetch_add(1)) < routed.size();) rcs[k] = msgpu_run(b->sys[routed[k]].ctx, &p);
+        };
+        std::vector<std::thread> pool;
+        const int nw = std::min<int>(kStreamWorkers, static_cast<int>(routed.size()));
+        for (int i = 0; i < nw; ++i) pool.emplace_back(worker);
+        for (auto &th : pool) th.join();
+        cudaSetDevice(b->device);
+    }
     cudaError_t e = cudaEventSynchronize(e1);
     float t = 0.f;
     cudaEventElapsedTime(&t, e0, e1);
@@ -243,12 +291,20 @@ int run_once(msgpu_batch *b, int ntimes, int m, int accumulate, long long step_o
     cudaEventDestroy(e1);
     if (rc) return rc;
     if (e) return bfail(b, MSGPU_ERR_CUDA, std::string("batch: run: ") + cudaGetErrorString(e));
+    for (size_t k = 0; k < routed.size(); ++k)
+        if (rcs[k])
+            return bfail(b, rcs[k], "batch: system " + std::to_string(routed[k]) + ": " +
+                                        msgpu_last_error(b->sys[routed[k]].ctx));
     int status = 0;
-    if ((e = cudaMemcpy(&status, b->status_d.p, sizeof(int), cudaMemcpyDeviceToHost)))
+    if (nitems > 0 && (e = cudaMemcpy(&status, b->status_d.p, sizeof(int), cudaMemcpyDeviceToHost)))
         return bfail(b, MSGPU_ERR_CUDA, std::string("batch: status: ") + cudaGetErrorString(e));
     if (status & 2) return bfail(b, MSGPU_ERR_NONFINITE, "batch: non-finite observable on the device");
     if (status & 1) return bfail(b, MSGPU_ERR_EXPM, "batch: small matrix exponential failed");
-    if (ms) *ms = t;
+    // persistent launch alone: its device time; with streamed systems: the
+    // wall time of the whole run (host threads, several streams)
+    if (ms)
+        *ms = routed.empty() ? t
+                             : std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - w0).count();
     return MSGPU_OK;
 }
 
@@ -279,6 +335,7 @@ void msgpu_batch_destroy(msgpu_batch *b)
     for (auto &s : b->sys) {
         Buf *all[] = {&s.rowptr, &s.col, &s.valf, &s.obs, &s.rates, &s.psi, &s.acc, &s.comp, &s.prev, &s.pflip};
         for (Buf *x : all) brelease(b, *x);
+        if (s.ctx) msgpu_destroy(s.ctx);
     }
     Buf *all[] = {&b->sys_d, &b->items_d, &b->queue_d, &b->status_d, &b->scratch, &b->times_d, &b->backup};
     for (Buf *x : all) brelease(b, *x);
@@ -300,6 +357,40 @@ int msgpu_batch_add_system(msgpu_batch *b, int dim, const int *rowptr, const int
     if (lo <= 0 || hi == lo || hi % (2 * lo) || dim % (2 * hi))
         return -bfail(b, MSGPU_ERR_INVALID, "batch: electron strides do not belong to two spin-1/2 digits");
     cudaSetDevice(b->device);
+    for (int k = 0; k < rowptr[dim]; ++k)
+        if (col[k] < 0 || col[k] >= dim || !std::isfinite(val[2 * k]) || !std::isfinite(val[2 * k + 1]))
+            return -bfail(b, MSGPU_ERR_INVALID, "batch: malformed Hamiltonian");
+    if (dim >= kStreamDim) {
+        // streamed single-system path: own context (charged to the batch budget)
+        const size_t room = b->budget ? (b->budget > b->used ? b->budget - b->used : 1) : 0;
+        msgpu_ctx *c = msgpu_create(b->device, room);
+        if (!c) return -bfail(b, MSGPU_ERR_CUDA, "batch: cannot create a context for a large system");
+        int rc = msgpu_upload_hamiltonian_csr(c, dim, rowptr, col, val);
+        if (!rc) rc = msgpu_set_reaction_scalar(c, kappa);
+        if (!rc) rc = msgpu_set_electron_pair(c, stride1, stride2);
+        for (int o = 0; o < nobs && !rc; ++o) rc = msgpu_add_pair_observable(c, ops + 32 * static_cast<size_t>(o), rates[o]);
+        if (!rc && st_rate > 0.0) rc = msgpu_set_st_noise(c, st_rate, MSGPU_NOISE_PHILOX, seed, nullptr, 0, 0);
+        if (!rc) rc = msgpu_upload_factors(c, dim, ntraj, factors);
+        if (rc) {
+            const std::string why = msgpu_last_error(c);
+            msgpu_destroy(c);
+            return -bfail(b, rc, "batch: " + why);
+        }
+        BatchSystem s;
+        s.D = dim;
+        s.M = ntraj;
+        s.nobs = nobs;
+        s.s1 = std::max(stride1, stride2);
+        s.s2 = std::min(stride1, stride2);
+        s.kappa = kappa;
+        s.st_rate = st_rate;
+        s.seed = seed;
+        s.ctx = c;
+        b->sys.push_back(s);
+        drop_graph(b);
+        b->tuned = 0;
+        return static_cast<int>(b->sys.size()) - 1;
+    }
     BatchSystem s;
     s.D = dim;
     s.M = ntraj;
@@ -357,10 +448,11 @@ int msgpu_batch_tune(msgpu_batch *b, const double *times, int ntimes, int krylov
     cudaSetDevice(b->device);
     // back up every state, time a short run per candidate, restore
     size_t total = 0;
-    for (auto &s : b->sys) total += s.psi.bytes;
+    for (auto &s : b->sys) total += s.psi.bytes;  // streamed systems hold no state here
     if (int rc = bensure(b, b->backup, total, "tuning backup")) return rc;
     size_t off = 0;
     for (auto &s : b->sys) {
+        if (!s.psi.bytes) continue;
         cudaMemcpyAsync(static_cast<char *>(b->backup.p) + off, s.psi.p, s.psi.bytes, cudaMemcpyDeviceToDevice, b->stream);
         off += s.psi.bytes;
     }
@@ -380,6 +472,7 @@ int msgpu_batch_tune(msgpu_batch *b, const double *times, int ntimes, int krylov
         }
     off = 0;
     for (auto &s : b->sys) {
+        if (!s.psi.bytes) continue;
         cudaMemcpyAsync(s.psi.p, static_cast<char *>(b->backup.p) + off, s.psi.bytes, cudaMemcpyDeviceToDevice, b->stream);
         off += s.psi.bytes;
     }
@@ -399,7 +492,8 @@ int msgpu_batch_run(msgpu_batch *b, const double *times, int ntimes, int krylov_
     cudaSetDevice(b->device);
     if (int rc = set_times(b, times, ntimes)) return rc;
     b->m = krylov_dim;
-    return run_once(b, ntimes, krylov_dim, accumulate, step_offset, b->threshold, b->ctas_per_sm, true, &b->last_ms);
+    return run_once(b, ntimes, krylov_dim, accumulate, step_offset, b->threshold, b->ctas_per_sm, true, &b->last_ms,
+                    times);
 }
 
 int msgpu_batch_fetch_yields(msgpu_batch *b, int system, double *per_traj, double *ensemble)
@@ -407,6 +501,10 @@ int msgpu_batch_fetch_yields(msgpu_batch *b, int system, double *per_traj, doubl
     if (!b) return MSGPU_ERR_INVALID;
     if (system < 0 || system >= static_cast<int>(b->sys.size())) return bfail(b, MSGPU_ERR_INVALID, "batch: no such system");
     BatchSystem &s = b->sys[system];
+    if (s.ctx) {
+        const int rc = msgpu_fetch_yields(s.ctx, per_traj, ensemble);
+        return rc ? bfail(b, rc, std::string("batch: ") + msgpu_last_error(s.ctx)) : MSGPU_OK;
+    }
     std::vector<double> acc(static_cast<size_t>(s.nobs) * s.M);
     if (cudaMemcpy(acc.data(), s.acc.p, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
         return bfail(b, MSGPU_ERR_CUDA, "batch: fetch failed");
@@ -420,6 +518,15 @@ int msgpu_batch_fetch_yields(msgpu_batch *b, int system, double *per_traj, doubl
         if (ensemble) ensemble[o] = sum;
     }
     return MSGPU_OK;
+}
+
+long long msgpu_batch_launch_count(const msgpu_batch *b)
+{
+    if (!b) return 0;
+    long long n = b->launches;
+    for (const auto &s : b->sys)
+        if (s.ctx) n += msgpu_launch_count(s.ctx);
+    return n;
 }
 
 int msgpu_batch_stats(const msgpu_batch *b, double *last_run_ms, int *team_threshold, int *ctas_per_sm)

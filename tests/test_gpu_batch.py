@@ -7,6 +7,7 @@ within 1e-6 of the largest per-trajectory yield of the complex128 oracle.
 import numpy as np
 import pytest
 
+from molspin_b200 import _lib as L
 from molspin_b200 import batching as B
 from molspin_b200 import hsgeneral as hs
 from molspin_b200 import systems as S
@@ -63,3 +64,31 @@ def test_batch_result_independent_of_companions_and_chunks():
     chunked, _ = _run(entries, times, 10, chunks=[7, 20])
     for x, y in zip(mixed, chunked):
         np.testing.assert_array_equal(x[0], y[0])
+
+
+def test_batch_streams_large_systems_through_the_single_system_path():
+    # D = 2048 reaches the streamed threshold: it runs on its own context
+    # beside the persistent launch, and equals the single-system complex64 run
+    big = h.random_system([2] * 5, [2] * 4, seed=54, st_rate=0.03, hf_scale=2.0, aniso=False)
+    assert big.dim == 2048
+    entries = [_systems()[0], (big, 45, 14)]
+    times = S.time_grid(12.0, 1.0)
+    m = 10
+    out, _ = _run(entries, times, m, tune=True)
+    F = big.trace_samples(45, 14.0)
+    with hs.HSPropagatorB200(0) as p:
+        p.set_hamiltonian(*big.hamiltonian_csr())
+        p.set_reaction(kappa=big.kappa())
+        p.set_electron_pair(*big.electron_strides())
+        p.set_observables([(op, rate) for _, op, rate in big.observables()])
+        p.set_noise(big.st_rate, L.NOISE_PHILOX, 14)
+        p.set_factors(F)
+        p.propagate(times, m, "c64")
+        per, ens = p.yields()
+    np.testing.assert_array_equal(out[1][0], per)
+    np.testing.assert_array_equal(out[1][1], ens)
+    bits = hs.philox_flip_bits(14, big.st_rate, times, 45)
+    ref = orc.hs_stochastic(big.hamiltonian_csr(), F, times, h.oracle_observables(big), kappa=big.kappa(), krylov=m,
+                            U_csr=orc.st_unitary(big.mult, 0, 1), event_rate=0.5 * big.st_rate, noise_mode=1,
+                            flip_bits=bits, nthreads=8)
+    assert np.max(np.abs(out[1][0] - ref["traj_yield"])) <= 1e-6 * np.max(np.abs(ref["traj_yield"]))
