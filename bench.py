@@ -247,8 +247,10 @@ def run_ours(args):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
-    ldm = (M + 63) // 64 * 64
     alg_bytes = 2 * D * M * 8 + len(col) * 12 + 4 * (D + 1)
+    # DRAM bytes per launch of this kernel at this workload (dram__bytes_read.sum
+    # + dram__bytes_write.sum of one ncu capture: 138.4 MB + 105.5 MB)
+    traffic = 243.9e6 if (D, M) == (16384, 1024) else None
     apply_avg_s = apply_ms / max(1, apply_n) / 1e3
     achieved = alg_bytes / apply_avg_s / 1e9 if apply_n else None
 
@@ -314,8 +316,8 @@ def run_ours(args):
                        "krylov": w.krylov, "dt_ns": w.dt, "time_steps_per_bench_step": chunk,
                        "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos",
                        "parallelism": f"independent trajectory blocks x{world}"},
-            "roofline": {"bound": "hbm", "kernel": "k_lanczos_apply", "achieved": achieved, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "k_lanczos_apply_compact", "achieved": achieved, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": traffic,
                          "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": apply_avg_s * 1e3, "launches": apply_n,
                          "share_of_step": apply_ms / el_ms if el_ms else None},
@@ -489,6 +491,9 @@ def run_dense(args):
     achieved = flops / (gms / gn / 1e3) / 1e12 if gn else None
     peaks = _peaks()
     peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    # DRAM bytes per GEMM launch from one ncu capture (bf16x3, D=1024, M=4096:
+    # 55.1 MB read + 6.8 MB written; the output stays partly in L2)
+    traffic = 61.9e6 if (D, M, prec) == (1024, 4096, "bf16x3") else None
     # accuracy against the complex128 Krylov path on a 256-trajectory subset
     sub = min(256, M)
     Fs = np.ascontiguousarray(F[:, :sub])
@@ -520,7 +525,7 @@ def run_dense(args):
         "config": {"workload": w.name, "trajectories_per_gpu": M, "time_steps_per_bench_step": chunk,
                    "renormalize": "exact Haberkorn survival", "l2": "state 2 x 33 MiB + U 16-24 MiB per step"},
         "roofline": {"bound": "tensor", "kernel": "k_dense_gemm", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak if achieved else None, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / peak if achieved else None, "traffic": traffic,
                      "peak_kind": "measured sustained" if "bf16_tflops_sustained" in peaks else "fallback",
                      "flops_per_launch": flops, "avg_launch_ms": gms / gn if gn else None,
                      "share_of_step": gms / el if el else None},
