@@ -84,7 +84,8 @@ struct msgpu_ctx {
     std::vector<double> last_values;
     int last_ntimes = 0;
     // profiling
-    bool prof = false;
+    int prof = 0;                   // 0 off, 1 every launch, 2 sampled (see msgpu_profile_enable)
+    long long prof_tick = -1;       // time step being issued (-1 outside the step loop)
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
     double prof_ms[KC_N] = {0};
     long long prof_n[KC_N] = {0};
@@ -139,21 +140,34 @@ int device_guard(msgpu_ctx *c)
     return MSGPU_OK;
 }
 
+// Sampled profiling times every launch of every kProfileEvery-th time step:
+// an event between two kernels costs them their overlap, so timing every
+// launch of every step slows a many-launch step by about 10 %, and timing
+// one step in kProfileEvery about 1 %.  (The first launch of a class in a
+// step is not representative: the first SpMM after the combine runs slower.)
+constexpr int kProfileEvery = 8;
+
 struct Timed {
     msgpu_ctx *c;
     int cls;
+    bool on = false;
     cudaEvent_t a = nullptr, b = nullptr;
     Timed(msgpu_ctx *c_, int cls_) : c(c_), cls(cls_)
     {
         ++c->launches;
-        if (!c->prof) return;
+        if (c->prof == 1) {
+            on = true;
+        } else if (c->prof == 2 && c->prof_tick >= 0 && c->prof_tick % kProfileEvery == 0) {
+            on = true;
+        }
+        if (!on) return;
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaEventRecord(a, c->stream);
     }
     ~Timed()
     {
-        if (!c->prof) return;
+        if (!on) return;
         cudaEventRecord(b, c->stream);
         c->ev.push_back({cls, {a, b}});
     }
@@ -648,7 +662,8 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
     float gemm_ms = 0.f;
     long long gemm_n = 0;
     c->launches += 2LL * (p->ntimes - 1) + 4;  // GEMM + epilogue per step; first epilogue, last values, two layout copies
-    if ((rc = msgpu::dense_run(c->dense, run, c->psi128.p, ldm, st, err, c->prof ? &gemm_ms : nullptr, &gemm_n)))
+    if ((rc = msgpu::dense_run(c->dense, run, c->psi128.p, ldm, st, err, c->prof ? &gemm_ms : nullptr, &gemm_n,
+                               c->prof == 2 ? kProfileEvery : 1)))
         return fail(c, rc, err);
     if (c->prof) {
         c->prof_ms[KC_GEMM] += gemm_ms;
@@ -951,24 +966,34 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    float best = 1e30f;
-    int best_qt = 32, best_v = 0;
+    // three interleaved rounds over all candidates, each candidate scored by
+    // its best round: a one-off delay (another stream, a profiler) then cannot
+    // pick the shape
+    std::vector<std::pair<int, int>> cands;
     for (int v = 0; v < kNumApplyVariants; ++v)
-        for (int qt : cand) {
-            if (qt > Q && qt != cand[0]) continue;
+        for (int qt : cand)
+            if (qt <= Q || qt == cand[0]) cands.push_back({v, qt});
+    std::vector<float> score(cands.size(), 1e30f);
+    for (int round = 0; round < 3; ++round)
+        for (size_t k = 0; k < cands.size(); ++k) {
+            const int v = cands[k].first, qt = cands[k].second;
             dim3 grid(ceil_div(Q, qt), c->ldm / 64);
             kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
                                                                 c->ldm, qt);
             cudaEventRecord(a, c->stream);
-            for (int rep = 0; rep < 3; ++rep)
+            for (int rep = 0; rep < 2; ++rep)
                 kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
                                                                     c->ldm, qt);
             cudaEventRecord(b, c->stream);
             cudaEventSynchronize(b);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, a, b);
-            if (ms < best) { best = ms; best_qt = qt; best_v = v; }
+            score[k] = std::min(score[k], ms);
         }
+    size_t pick = 0;
+    for (size_t k = 1; k < cands.size(); ++k)
+        if (score[k] < score[pick]) pick = k;
+    const int best_v = cands[pick].first, best_qt = cands[pick].second;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaError_t e = cudaGetLastError();
@@ -1019,6 +1044,7 @@ int msgpu_download_factors(msgpu_ctx *c, double *factors)
 int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
 {
     if (!c) return MSGPU_ERR_INVALID;
+    c->prof_tick = -1;
     if (!p || !p->times || p->ntimes < 1) return fail(c, MSGPU_ERR_INVALID, "run: a time grid with at least one point is required");
     if (c->D == 0) return fail(c, MSGPU_ERR_STATE, "run: no Hamiltonian uploaded");
     if (c->state_prec < 0) return fail(c, MSGPU_ERR_STATE, "run: no trajectory factors uploaded");
@@ -1152,6 +1178,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         return cuda_fail(c, e, "expm shared memory");
 
     for (int s = 0; s < steps; ++s) {
+        c->prof_tick = s;
         const double dt = p->times[s + 1] - p->times[s];
         const long long g = g0 + s;
         if ((e = cudaMemsetAsync(c->mdim.p, 0, ldm * sizeof(int), st))) return cuda_fail(c, e, "mdim reset");
@@ -1248,9 +1275,9 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             }
             {
                 Timed tm(c, KC_EXPM);
-                k_krylov_expm<<<ceil_div(ldm, expm_warps), 32 * expm_warps, expm_warps * expm_smem_warp, st>>>(
-                    nullptr, td, to, kappa, static_cast<int *>(c->mdim.p), beta0, sc, mws, ldm, M, dt,
-                    static_cast<double2 *>(c->coef.p), static_cast<int *>(c->status.p));
+                k_lanczos_expm<<<ceil_div(ldm, 8), 256, 0, st>>>(td, to, kappa, static_cast<int *>(c->mdim.p), beta0,
+                                                                sc, mws, ldm, M, dt, static_cast<double2 *>(c->coef.p),
+                                                                static_cast<int *>(c->status.p));
             }
             {
                 Timed tm(c, KC_COMBINE);
@@ -1263,6 +1290,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         yield_update(dt, 0, s + 1);
         if ((e = cudaGetLastError())) return cuda_fail(c, e, "step launch");
     }
+    c->prof_tick = -1;
     int status = 0;
     c->last_values.assign(static_cast<size_t>(p->ntimes) * nobs, 0.0);
     if ((e = cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
@@ -1312,7 +1340,8 @@ int msgpu_fetch_values(msgpu_ctx *c, double *values)
 int msgpu_profile_enable(msgpu_ctx *c, int enable)
 {
     if (!c) return MSGPU_ERR_INVALID;
-    c->prof = enable != 0;
+    if (enable < 0 || enable > 2) return fail(c, MSGPU_ERR_INVALID, "profile: mode must be 0, 1 or 2");
+    c->prof = enable;
     for (int k = 0; k < KC_N; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
     return MSGPU_OK;
 }

@@ -759,7 +759,7 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
 }
 
 int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaStream_t stream, std::string &err,
-              float *gemm_ms, long long *gemm_launches)
+              float *gemm_ms, long long *gemm_launches, int gemm_every)
 {
     const int D = st.D, Dp = st.Dp, M = st.M, Mp = st.Mp, ns = st.parts;
     CUtensorMap ta[3], tb[3];
@@ -845,23 +845,24 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     E.prev_tvals = nullptr;
     E.prev_values = nullptr;
     k_dense_epilogue<<<Mp, kEpiThreads, epi_smem, stream>>>(static_cast<float *>(st.psi), bp, E);
-    // GEMM launches are bracketed by events only when timing was requested;
-    // the events are read after the loop so the host never waits per step.
-    std::vector<cudaEvent_t> evs;
-    if (gemm_ms) {
-        evs.resize(2 * static_cast<size_t>(steps));
-        for (auto &ev : evs) cudaEventCreate(&ev);
-    }
+    // GEMM launches are bracketed by events only when timing was requested,
+    // every gemm_every-th step (an event between two kernels costs them their
+    // overlap); the events are read after the loop so the host never waits.
+    gemm_every = std::max(1, gemm_every);
+    const int ntimed = gemm_ms ? (steps + gemm_every - 1) / gemm_every : 0;
+    std::vector<cudaEvent_t> evs(2 * static_cast<size_t>(ntimed));
+    for (auto &ev : evs) cudaEventCreate(&ev);
     dim3 grid(Mp / BN, Dp / kGM);
     for (int s = 0; s < steps; ++s) {
-        if (gemm_ms) cudaEventRecord(evs[2 * s], stream);
+        const bool timed = gemm_ms && s % gemm_every == 0;
+        if (timed) cudaEventRecord(evs[2 * (s / gemm_every)], stream);
         if (ns == 2)
             k_dense_gemm<2><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
                                                                static_cast<float *>(st.psi), Dp, run.status);
         else
             k_dense_gemm<3><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
                                                                static_cast<float *>(st.psi), Dp, run.status);
-        if (gemm_ms) cudaEventRecord(evs[2 * s + 1], stream);
+        if (timed) cudaEventRecord(evs[2 * (s / gemm_every) + 1], stream);
         E.stepA = run.step_offset + s;
         E.halfA = 1;
         E.pA = pstep(s);
@@ -885,15 +886,15 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     if (gemm_ms) {
         float total = 0.f;
         if (!evs.empty()) cudaEventSynchronize(evs.back());
-        for (int s = 0; s < steps; ++s) {
+        for (int k = 0; k < ntimed; ++k) {
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, evs[2 * s], evs[2 * s + 1]);
+            cudaEventElapsedTime(&ms, evs[2 * k], evs[2 * k + 1]);
             total += ms;
         }
-        for (auto &ev : evs) cudaEventDestroy(ev);
         *gemm_ms = total;
     }
-    if (gemm_launches) *gemm_launches = steps;
+    for (auto &ev : evs) cudaEventDestroy(ev);
+    if (gemm_launches) *gemm_launches = gemm_ms ? ntimed : steps;  // launches the time covers
     // ensemble values of the last time point
     k_dense_values<<<run.nobs, kEpiThreads, 0, stream>>>(tv[steps & 1], M, run.nobs,
                                                          run.values + static_cast<size_t>(steps) * run.nobs);

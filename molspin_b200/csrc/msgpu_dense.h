@@ -63,7 +63,7 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
 // Runs the time loop; returns MSGPU_* status (err filled on failure); the
 // final state is written back to psi128_interleaved.
 int dense_run(DenseState &st, const DenseRun &run, void *psi128_interleaved, int ldm, cudaStream_t stream,
-              std::string &err, float *gemm_ms, long long *gemm_launches);
+              std::string &err, float *gemm_ms, long long *gemm_launches, int gemm_every = 1);
 
 void dense_release(DenseState &st, void (*release)(void *ctx, void *p), void *ctx);
 

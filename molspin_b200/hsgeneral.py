@@ -185,8 +185,10 @@ class HSPropagatorB200:
     def launch_count(self) -> int:
         return int(L.lib.msgpu_launch_count(self.ctx))
 
-    def profile(self, enable: bool = True):
-        _check(self.ctx, L.lib.msgpu_profile_enable(self.ctx, 1 if enable else 0))
+    def profile(self, enable: bool | int = True):
+        """True/1: time every launch; 2: sampled (every 8th time step); False/0: off."""
+        mode = int(enable) if not isinstance(enable, bool) else (1 if enable else 0)
+        _check(self.ctx, L.lib.msgpu_profile_enable(self.ctx, mode))
 
     def profile_read(self, cls: int):
         ms = C.c_double(0.0)
