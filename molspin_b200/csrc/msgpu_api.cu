@@ -49,7 +49,7 @@ struct msgpu_ctx {
     int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
     // resident (one warp per trajectory, whole time loop per launch) form
     int form = MSGPU_FORM_AUTO;
-    DevBuf colbuf, trajval, times_d, pflip_d, sys_d, work_d, obs_d;
+    DevBuf colbuf, trajval, times_d, pflip_d, sys_d, work_d, obs_d, dense_part;
     // dense tensor-core form
     msgpu::DenseState dense;
     std::vector<std::pair<void *, size_t>> dense_allocs;
@@ -215,6 +215,7 @@ PairObs make_pair_obs(const msgpu_ctx *c)
     return po;
 }
 
+void dense_release_cb(void *ctx, void *p);  // defined with the dense form below
 }  // namespace
 
 extern "C" {
@@ -247,8 +248,10 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
-                     &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d};
+                     &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d,
+                     &c->dense_part};
     for (DevBuf *b : all) release(c, *b);
+    msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
     for (auto &a : c->dense_allocs) cudaFree(a.first);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -602,7 +605,8 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
         (rc = ensure(c, c->rates_d, 8 * sizeof(double), "rates")) ||
         (rc = ensure(c, c->status, sizeof(int), "status")) ||
         (rc = ensure(c, c->values_d, static_cast<size_t>(p->ntimes) * nobs * sizeof(double), "values")) ||
-        (rc = ensure(c, c->obs_d, 8 * 16 * sizeof(double2), "observables")))
+        (rc = ensure(c, c->obs_d, 8 * 16 * sizeof(double2), "observables")) ||
+        (rc = ensure(c, c->dense_part, 2 * static_cast<size_t>(p->ntimes) * nobs * sizeof(double), "dense values")))
         return rc;
     const PairObs po = make_pair_obs(c);
     cudaError_t e;
@@ -649,6 +653,7 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
     run.st_rate = c->st_rate;
     run.renormalize = c->dense_renorm;
     run.status = static_cast<int *>(c->status.p);
+    run.part = static_cast<double *>(c->dense_part.p);
     const int parts = p->precision == MSGPU_PREC_BF16X6 ? 3 : 2;
     const double dt = p->ntimes > 1 ? p->times[1] - p->times[0] : 1.0;
     for (int s = 1; s + 1 < p->ntimes; ++s)

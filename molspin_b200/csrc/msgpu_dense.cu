@@ -152,13 +152,14 @@ __device__ __forceinline__ void umma_commit(uint32_t bar)
 //   A parts: Dp x Dp BF16, row-major (K contiguous)  -> tensor maps ta[0..NS)
 //   B parts: Mp x Dp BF16, row-major (K contiguous)  -> tensor maps tb[0..NS)
 //   out:     Mp x Dp FP32, out[n][m] = C[m][n]
-// grid = (Mp / BN, Dp / 128), block = 128 threads.
+// grid = (trajectory tiles of this launch, Dp / 128), block = 128 threads;
+// the launch covers the trajectory tiles from n_tile0 on.
 template <int NS>
 __global__ void __launch_bounds__(kGThreads, 1)
 k_dense_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
              const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
              const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2, float *__restrict__ out,
-             int Dp, int *__restrict__ status)
+             int Dp, int n_tile0, int *__restrict__ status)
 {
     using Cfg = GemmCfg<NS>;
     constexpr int BN = Cfg::BN;
@@ -172,7 +173,7 @@ k_dense_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CU
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ptr + 9);
     const uint32_t full0 = bars, empty0 = bars + 16, accum = bars + 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kGM;
+    const int n0 = (n_tile0 + blockIdx.x) * BN, m0 = blockIdx.y * kGM;
     const int nk = Dp / kGK;
     const CUtensorMap *ta[3] = {&ta0, &ta1, &ta2};
     const CUtensorMap *tb[3] = {&tb0, &tb1, &tb2};
@@ -430,6 +431,7 @@ struct DenseEpi {
     double elapsed;       // t - t0 of this time point
     int renormalize;
     int store_state;            // write the FP32 state back (last time point of a run)
+    int t0, t1;                 // this launch's trajectories [t0, t1) (one stream group)
     const double *prev_tvals;   // previous time point's per-trajectory values, or null
     double *prev_values;        // its ensemble values (nobs doubles)
     int *status;
@@ -451,12 +453,12 @@ __device__ __forceinline__ int dense_flip(const DenseEpi &E, int t, long long st
 
 // Ensemble value of one observable: the sum over trajectories of tvals[t][o]
 // in a fixed order (256 threads, strided partial sums, warp tree, warp order).
-__device__ __forceinline__ double dense_ensemble_sum(const double *__restrict__ tvals, int M, int nobs, int o,
+__device__ __forceinline__ double dense_ensemble_sum(const double *__restrict__ tvals, int t0, int t1, int nobs, int o,
                                                     double (*red)[8])
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double a = 0.0;
-    for (int t = threadIdx.x; t < M; t += blockDim.x) a += tvals[static_cast<size_t>(t) * nobs + o];
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) a += tvals[static_cast<size_t>(t) * nobs + o];
     a = warp_sum(a);
     if (lane == 0) red[0][warp] = a;
     __syncthreads();
@@ -481,7 +483,7 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
     __shared__ double red[9][8];
     __shared__ double s_scale;
     __shared__ double2 s_obs[8][10];
-    const int t = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = E.t0 + blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *col = psi + static_cast<size_t>(t) * E.Dp;
     if (threadIdx.x < 80) s_obs[threadIdx.x / 10][threadIdx.x % 10] = E.obs_c[threadIdx.x / 10][threadIdx.x % 10];
     const int n4 = E.D / 2;
@@ -625,18 +627,29 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
     }
     if (E.prev_tvals && blockIdx.x < E.nobs) {
         __syncthreads();  // red[0] is reused below
-        const double v = dense_ensemble_sum(E.prev_tvals, E.M, E.nobs, blockIdx.x, red);
+        const double v = dense_ensemble_sum(E.prev_tvals, E.t0, min(E.t1, E.M), E.nobs, blockIdx.x, red);
         if (threadIdx.x == 0) E.prev_values[blockIdx.x] = v;
     }
 }
 
-// values[o] = ensemble value of the last time point (same order as above)
-__global__ void __launch_bounds__(kEpiThreads) k_dense_values(const double *__restrict__ tvals, int M, int nobs,
-                                                              double *__restrict__ values)
+// values[o] = one group's part of the last time point's ensemble value
+// (same order as above)
+__global__ void __launch_bounds__(kEpiThreads) k_dense_values(const double *__restrict__ tvals, int t0, int t1,
+                                                              int nobs, double *__restrict__ values)
 {
     __shared__ double red[9][8];
-    const double v = dense_ensemble_sum(tvals, M, nobs, blockIdx.x, red);
+    const double v = dense_ensemble_sum(tvals, t0, t1, nobs, blockIdx.x, red);
     if (threadIdx.x == 0) values[blockIdx.x] = v;
+}
+
+// values[i] = sum over the stream groups of their parts, in group order
+__global__ void k_dense_sum_groups(const double *__restrict__ part, int groups, size_t n, double *__restrict__ values)
+{
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = 0.0;
+    for (int g = 0; g < groups; ++g) v += part[static_cast<size_t>(g) * n + i];
+    values[i] = v;
 }
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -833,6 +846,48 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         return s < steps ? -0.5 * std::expm1(-2.0 * (0.5 * run.st_rate) * (0.5 * (run.times[s + 1] - run.times[s])))
                          : 0.0;
     };
+    // Two stream groups when the block has at least two trajectory tiles:
+    // group g owns tiles [gt[g], gt[g+1]) and runs its GEMM -> epilogue chain
+    // on its own stream, so one group's epilogue overlaps the other's GEMM
+    // (the groups share no data: a GEMM tile reads only its own trajectories).
+    const int Mt = Mp / BN;
+    const int G = Mt >= 2 ? 2 : 1;
+    const int gt[3] = {0, G == 2 ? Mt / 2 : Mt, Mt};
+    if (G == 2 && !st.side) {
+        if ((e = cudaStreamCreateWithFlags(&st.side, cudaStreamNonBlocking)) ||
+            (e = cudaEventCreateWithFlags(&st.e_main, cudaEventDisableTiming)) ||
+            (e = cudaEventCreateWithFlags(&st.e_side, cudaEventDisableTiming))) {
+            err = std::string("dense: second stream: ") + cudaGetErrorString(e);
+            return MSGPU_ERR_CUDA;
+        }
+    }
+    cudaStream_t ss[2] = {stream, G == 2 ? st.side : stream};
+    auto fork = [&]() {  // the side stream continues after everything issued on the main stream so far
+        cudaEventRecord(st.e_main, stream);
+        cudaStreamWaitEvent(st.side, st.e_main, 0);
+    };
+    auto join = [&]() {  // the main stream continues after everything issued on the side stream so far
+        cudaEventRecord(st.e_side, st.side);
+        cudaStreamWaitEvent(stream, st.e_side, 0);
+    };
+    const size_t nv = static_cast<size_t>(run.ntimes) * run.nobs;  // one group's partial values
+    auto epilogue = [&](int g, long long point_prev) {
+        DenseEpi Eg = E;
+        Eg.t0 = gt[g] * BN;
+        Eg.t1 = gt[g + 1] * BN;
+        Eg.prev_values = point_prev >= 0 ? run.part + g * nv + static_cast<size_t>(point_prev) * run.nobs : nullptr;
+        k_dense_epilogue<<<Eg.t1 - Eg.t0, kEpiThreads, epi_smem, ss[g]>>>(static_cast<float *>(st.psi), bp, Eg);
+    };
+    auto gemm = [&](int g, cudaStream_t sg) {
+        dim3 grid(gt[g + 1] - gt[g], Dp / kGM);
+        if (ns == 2)
+            k_dense_gemm<2><<<grid, kGThreads, smem, sg>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
+                                                           static_cast<float *>(st.psi), Dp, gt[g], run.status);
+        else
+            k_dense_gemm<3><<<grid, kGThreads, smem, sg>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
+                                                           static_cast<float *>(st.psi), Dp, gt[g], run.status);
+    };
+    if (G == 2) fork();
     // first time point: evaluate, first half-step flip of step 0, split
     E.stepA = steps > 0 ? run.step_offset : -1;
     E.halfA = 0;
@@ -843,26 +898,25 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     E.elapsed = 0.0;
     E.store_state = steps == 0;
     E.prev_tvals = nullptr;
-    E.prev_values = nullptr;
-    k_dense_epilogue<<<Mp, kEpiThreads, epi_smem, stream>>>(static_cast<float *>(st.psi), bp, E);
-    // GEMM launches are bracketed by events only when timing was requested,
-    // every gemm_every-th step (an event between two kernels costs them their
-    // overlap); the events are read after the loop so the host never waits.
+    for (int g = 0; g < G; ++g) epilogue(g, -1);
+    // GEMMs are bracketed by events only when timing was requested, every
+    // gemm_every-th step (an event between two kernels costs them their
+    // overlap).  On a timed step both groups' GEMMs run back to back on the
+    // main stream, so a timed launch is one GEMM over the whole block; the
+    // events are read after the loop so the host never waits.
     gemm_every = std::max(1, gemm_every);
     const int ntimed = gemm_ms ? (steps + gemm_every - 1) / gemm_every : 0;
     std::vector<cudaEvent_t> evs(2 * static_cast<size_t>(ntimed));
     for (auto &ev : evs) cudaEventCreate(&ev);
-    dim3 grid(Mp / BN, Dp / kGM);
     for (int s = 0; s < steps; ++s) {
         const bool timed = gemm_ms && s % gemm_every == 0;
-        if (timed) cudaEventRecord(evs[2 * (s / gemm_every)], stream);
-        if (ns == 2)
-            k_dense_gemm<2><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
-                                                               static_cast<float *>(st.psi), Dp, run.status);
-        else
-            k_dense_gemm<3><<<grid, kGThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
-                                                               static_cast<float *>(st.psi), Dp, run.status);
-        if (timed) cudaEventRecord(evs[2 * (s / gemm_every) + 1], stream);
+        if (timed) {
+            if (G == 2) join();
+            cudaEventRecord(evs[2 * (s / gemm_every)], stream);
+            for (int g = 0; g < G; ++g) gemm(g, stream);
+            cudaEventRecord(evs[2 * (s / gemm_every) + 1], stream);
+            if (G == 2) fork();
+        }
         E.stepA = run.step_offset + s;
         E.halfA = 1;
         E.pA = pstep(s);
@@ -873,16 +927,26 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         E.dt = run.times[s + 1] - run.times[s];
         E.elapsed = run.times[s + 1] - run.times[0];
         E.tvals = tv[(s + 1) & 1];
-        E.prev_tvals = tv[s & 1];  // time point s, summed by blocks 0..nobs-1
-        E.prev_values = run.values + static_cast<size_t>(s) * run.nobs;
+        E.prev_tvals = tv[s & 1];  // time point s, summed per group by blocks 0..nobs-1
         E.store_state = s + 1 == steps;
-        k_dense_epilogue<<<Mp, kEpiThreads, epi_smem, stream>>>(static_cast<float *>(st.psi), bp, E);
+        for (int g = 0; g < G; ++g) {
+            if (!timed) gemm(g, ss[g]);
+            epilogue(g, s);
+        }
         if ((e = cudaGetLastError())) {
             err = std::string("dense: step: ") + cudaGetErrorString(e);
+            if (G == 2) join();
             for (auto &ev : evs) cudaEventDestroy(ev);
             return MSGPU_ERR_CUDA;
         }
     }
+    // each group's part of the last time point, then the group sums
+    for (int g = 0; g < G; ++g)
+        k_dense_values<<<run.nobs, kEpiThreads, 0, ss[g]>>>(tv[steps & 1], gt[g] * BN, std::min(gt[g + 1] * BN, M),
+                                                            run.nobs,
+                                                            run.part + g * nv + static_cast<size_t>(steps) * run.nobs);
+    if (G == 2) join();
+    k_dense_sum_groups<<<static_cast<unsigned>((nv + 255) / 256), 256, 0, stream>>>(run.part, G, nv, run.values);
     if (gemm_ms) {
         float total = 0.f;
         if (!evs.empty()) cudaEventSynchronize(evs.back());
@@ -894,10 +958,7 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         *gemm_ms = total;
     }
     for (auto &ev : evs) cudaEventDestroy(ev);
-    if (gemm_launches) *gemm_launches = gemm_ms ? ntimed : steps;  // launches the time covers
-    // ensemble values of the last time point
-    k_dense_values<<<run.nobs, kEpiThreads, 0, stream>>>(tv[steps & 1], M, run.nobs,
-                                                         run.values + static_cast<size_t>(steps) * run.nobs);
+    if (gemm_launches) *gemm_launches = gemm_ms ? ntimed : steps;  // full-block GEMMs the time covers
     const size_t nc = static_cast<size_t>(D) * ldm;
     k_dense_to_ctx<<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const float *>(st.psi), D, M, ldm, Dp,
                                                        static_cast<double2 *>(psi128));
@@ -910,6 +971,12 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
 
 void dense_release(DenseState &st, void (*release)(void *ctx, void *p), void *ctx)
 {
+    if (st.side) {
+        cudaStreamSynchronize(st.side);
+        cudaStreamDestroy(st.side);
+    }
+    if (st.e_main) cudaEventDestroy(st.e_main);
+    if (st.e_side) cudaEventDestroy(st.e_side);
     release(ctx, st.u_parts);
     release(ctx, st.psi);
     release(ctx, st.b_parts);

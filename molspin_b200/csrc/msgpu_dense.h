@@ -22,6 +22,10 @@ struct DenseState {
     void *work = nullptr;     // FP64 scratch for building U (4 x D x D complex)
     void *tmaps = nullptr;    // device copy not needed: tensor maps are kernel parameters
     size_t bytes = 0;
+    // second trajectory group: its GEMMs and epilogues run on `side`, so one
+    // group's epilogue overlaps the other group's GEMM
+    cudaStream_t side = nullptr;
+    cudaEvent_t e_main = nullptr, e_side = nullptr;
 };
 
 // Arguments of the dense run that come from the context.
@@ -51,6 +55,7 @@ struct DenseRun {
     double st_rate;
     int renormalize;            // restore the exact Haberkorn survival norm each step (scalar K only)
     int *status;                // device status word
+    double *part;               // device: 2 x ntimes x nobs per-group ensemble partials
 };
 
 // Allocates (budget-checked by the caller through *alloc) and prepares the
