@@ -64,6 +64,55 @@ __device__ __forceinline__ int quartet_base(int q, int s1, int s2)
     return hi * (2 * s1) + mid * (2 * s2) + lo;
 }
 
+// Lanczos form (K = kappa I, H Hermitian): the Krylov matrix is
+// dt (-kappa I - i T) with T real symmetric tridiagonal, so its exponential
+// applied to e1 is e^{-kappa dt} exp(-i dt T) e1.  Lane i < n supplies T_ii
+// (diag), T_i,i-1 (lo; 0 on lane 0) and T_i,i+1 (hi; 0 on lane n-1); every
+// lane of the warp must call.  exp(B) e1 with B = -i dt T is taken as r equal
+// sub-steps exp(B / r), r = ceil(||B||_inf / 4), each a Taylor series whose
+// degree K is the smallest with theta^(K+1) / (K+1)! < 1e-17,
+// theta = ||B||_inf / r (terms never exceed 4^4/4!, so the cancellation costs
+// about one digit); the tridiagonal matvec is two warp shuffles.  Lane i
+// returns y_i (0 for i >= n); false on a non-finite result or a norm beyond
+// 4 x kTridiagMaxSubsteps.
+constexpr int kTridiagMaxSubsteps = 1 << 14;
+
+__device__ inline bool warp_tridiag_expm_e1(int n, double diag, double lo, double hi, double kappa, double dt,
+                                            double2 &y)
+{
+    const int lane = threadIdx.x & 31;
+    const bool live = lane < n;
+    const double d = live ? -dt * diag : 0.0;
+    const double l = (live && lane > 0) ? -dt * lo : 0.0;
+    const double h = (lane + 1 < n) ? -dt * hi : 0.0;
+    const double nrm = warp_max(fabs(d) + fabs(l) + fabs(h));
+    y = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
+    if (!(isfinite(nrm) && nrm <= 4.0 * kTridiagMaxSubsteps)) return false;
+    const int r = max(1, static_cast<int>(ceil(nrm / 4.0)));
+    const double theta = nrm / r, inv_r = 1.0 / r;
+    int K = 1;
+    for (double rem = theta * theta / 2.0; rem >= 1e-17 && K < 64; ++K) rem *= theta / (K + 2);
+    const double ds = d * inv_r, ls = l * inv_r, hs = h * inv_r;
+    for (int rep = 0; rep < r; ++rep) {
+        double2 term = y, acc = y;
+        for (int k = 1; k <= K; ++k) {
+            // (B term)_i = i (l term_{i-1} + d term_i + h term_{i+1})
+            const double pr = __shfl_up_sync(0xffffffffu, term.x, 1), pi = __shfl_up_sync(0xffffffffu, term.y, 1);
+            const double nr = __shfl_down_sync(0xffffffffu, term.x, 1), ni = __shfl_down_sync(0xffffffffu, term.y, 1);
+            const double re = ls * pr + ds * term.x + hs * nr;
+            const double im = ls * pi + ds * term.y + hs * ni;
+            const double inv = 1.0 / k;
+            term = live ? make_double2(-im * inv, re * inv) : make_double2(0.0, 0.0);  // times i / k
+            acc.x += term.x;
+            acc.y += term.y;
+        }
+        y = acc;
+    }
+    const double sk = exp(-kappa * dt);
+    y = make_double2(y.x * sk, y.y * sk);
+    return __all_sync(0xffffffffu, isfinite(y.x) && isfinite(y.y));
+}
+
 // ------------------------------------------------------------ small expm
 // Per-warp matrix exponential of an n x n complex matrix (n <= 32) held in
 // shared memory, column-major, by scaling and squaring with the diagonal (6,6)

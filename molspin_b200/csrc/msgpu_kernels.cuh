@@ -500,18 +500,9 @@ __global__ void k_krylov_expm(const double2 *__restrict__ hess, const double *__
     if (!ok && lane == 0 && t < M) atomicOr(status, 1);
 }
 
-// Lanczos form (K = kappa I, H Hermitian): the Krylov matrix is
-// dt (-kappa I - i T) with T real symmetric tridiagonal (diagonal tdiag =
-// alpha, off-diagonal toff = beta), so exp(.) e1 = e^{-kappa dt} exp(-i dt T) e1.
-// One warp per trajectory, lane i holds component i; the tridiagonal matvec
-// is two warp shuffles.  exp(B) e1 with B = -i dt T is taken as r equal
-// sub-steps exp(B / r), r = ceil(||B||_inf / 4), each a Taylor series whose
-// degree K is the smallest with theta^(K+1) / (K+1)! < 1e-17,
-// theta = ||B||_inf / r (terms never exceed 4^4/4!, so the cancellation costs
-// about one digit).  Coefficients as in k_krylov_expm: coef[j][t] =
-// beta0 * vscale_j * y_j.
-constexpr int kLanczosMaxSubsteps = 1 << 14;
-
+// Krylov exponential of the Lanczos form (tridiagonal, see
+// warp_tridiag_expm_e1): one warp per trajectory.  Coefficients as in
+// k_krylov_expm: coef[j][t] = beta0 * vscale_j * y_j.
 __global__ void __launch_bounds__(256)
 k_lanczos_expm(const double *__restrict__ tdiag, const double *__restrict__ toff, double kappa,
                const int *__restrict__ mdim, const double *__restrict__ beta0, const double *__restrict__ vscale,
@@ -523,39 +514,15 @@ k_lanczos_expm(const double *__restrict__ tdiag, const double *__restrict__ toff
     const int n = max(1, mdim[t]);
     const double b0 = beta0[t];
     const bool live = lane < n;
-    const double d = live ? -dt * tdiag[static_cast<size_t>(t) * m + lane] : 0.0;                    // B_ii / i
-    const double lo = (live && lane > 0) ? -dt * toff[static_cast<size_t>(t) * m + lane - 1] : 0.0;  // B_i,i-1 / i
-    const double hi = (lane + 1 < n) ? -dt * toff[static_cast<size_t>(t) * m + lane] : 0.0;          // B_i,i+1 / i
-    const double nrm = warp_max(fabs(d) + fabs(lo) + fabs(hi));
-    bool ok = isfinite(nrm) && b0 > 0.0 && nrm <= 4.0 * kLanczosMaxSubsteps;
-    double2 y = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
-    if (ok) {
-        const int r = max(1, static_cast<int>(ceil(nrm / 4.0)));
-        const double theta = nrm / r, inv_r = 1.0 / r;
-        int K = 1;
-        for (double rem = theta * theta / 2.0; rem >= 1e-17 && K < 64; ++K) rem *= theta / (K + 2);
-        const double ds = d * inv_r, los = lo * inv_r, his = hi * inv_r;
-        for (int rep = 0; rep < r; ++rep) {
-            double2 term = y, acc = y;
-            for (int k = 1; k <= K; ++k) {
-                // (B term)_i = i (lo term_{i-1} + d term_i + hi term_{i+1})
-                const double pr = __shfl_up_sync(0xffffffffu, term.x, 1), pi = __shfl_up_sync(0xffffffffu, term.y, 1);
-                const double nr = __shfl_down_sync(0xffffffffu, term.x, 1), ni = __shfl_down_sync(0xffffffffu, term.y, 1);
-                const double re = los * pr + ds * term.x + his * nr;
-                const double im = los * pi + ds * term.y + his * ni;
-                const double inv = 1.0 / k;
-                term = live ? make_double2(-im * inv, re * inv) : make_double2(0.0, 0.0);  // times i / k
-                acc.x += term.x;
-                acc.y += term.y;
-            }
-            y = acc;
-        }
-        ok = isfinite(y.x) && isfinite(y.y);
-    }
+    const double d = live ? tdiag[static_cast<size_t>(t) * m + lane] : 0.0;
+    const double lo = (live && lane > 0) ? toff[static_cast<size_t>(t) * m + lane - 1] : 0.0;
+    const double hi = (lane + 1 < n) ? toff[static_cast<size_t>(t) * m + lane] : 0.0;
+    double2 y;
+    const bool ok = warp_tridiag_expm_e1(n, d, lo, hi, kappa, dt, y) && b0 > 0.0;
     if (lane < m) {
         double2 c = make_double2(0.0, 0.0);
         if (ok && live) {
-            c = cscale(y, b0 * exp(-kappa * dt));
+            c = cscale(y, b0);
             if (vscale) c = cscale(c, vscale[static_cast<size_t>(lane) * ldm + t]);
         }
         coef[static_cast<size_t>(lane) * ldm + t] = c;

@@ -268,17 +268,21 @@ __global__ void k_resident(const ResidentSystem *__restrict__ systems, const Res
                     __syncwarp();
                 }
                 __syncwarp();
-                if (lane < n)
-                    for (int i = 0; i < n; ++i) {
-                        double2 v = make_double2(0.0, 0.0);
-                        if (i == lane) v = make_double2(-S.kappa, -Hm[i].x);
-                        else if (i == lane + 1) v = make_double2(0.0, -Hm[lane].y);
-                        else if (i + 1 == lane) v = make_double2(0.0, -Hm[i].y);
-                        A[i + lane * n] = cscale(v, dt);
-                    }
             }
             __syncwarp();
-            const bool ok = warp_expm_col0(n, A, X, N, Dm, y);
+            bool ok;
+            if (kLanczos) {
+                // tridiagonal: alpha on Hm[i].x, beta_{i+1} on Hm[i].y
+                const double d = lane < n ? Hm[lane].x : 0.0;
+                const double lo = (lane < n && lane > 0) ? Hm[lane - 1].y : 0.0;
+                const double hi = lane + 1 < n ? Hm[lane].y : 0.0;
+                double2 yl;
+                ok = warp_tridiag_expm_e1(n, d, lo, hi, S.kappa, dt, yl);
+                if (lane < n) y[lane] = yl;
+                __syncwarp();
+            } else {
+                ok = warp_expm_col0(n, A, X, N, Dm, y);
+            }
             if (!ok) {
                 if (lane == 0) atomicOr(status, 1);
                 n = 0;
