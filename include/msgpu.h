@@ -108,6 +108,22 @@ int msgpu_set_stream(msgpu_ctx *ctx, void *cuda_stream);
  * values.  Replaces the sp_cx_mat passed to HSPropagator::Step (HSPropagator.h:40-41). */
 int msgpu_upload_hamiltonian_csr(msgpu_ctx *ctx, int dim, const int *rowptr, const int *col, const double *val);
 
+
+/* H as a fixed-pattern linear combination H = sum_k coef_k H_k, 1 <= nterms
+ * <= 16 (for example H_hf + Bx Zx + By Zy + Bz Zz: a new field direction or
+ * strength changes only the coefficients -- the per-orientation Hamiltonian
+ * of TaskHSGeneral.cpp:371-379 and SpinSpace_hamiltonians.cpp:780-1043 with
+ * a sparsity pattern that does not change).  The terms share one CSR pattern
+ * (rowptr, col; a term stores explicit zeros where the others have entries);
+ * vals holds nterms blocks of nnz interleaved complex values.  The derived
+ * device forms (complex64 copy, quartet blocks) are built once from the
+ * pattern; msgpu_set_hamiltonian_coefficients then updates H on the device,
+ * without host assembly or re-upload, and drops a cached dense propagator.
+ * msgpu_upload_hamiltonian_csr leaves this mode. */
+int msgpu_upload_hamiltonian_terms(msgpu_ctx *ctx, int dim, const int *rowptr, const int *col, int nterms,
+                                   const double *vals, const double *coef);
+int msgpu_set_hamiltonian_coefficients(msgpu_ctx *ctx, const double *coef);
+
 /* K = kappa * I (symmetric recombination: kappa = k/2,
  * HSReactionRelaxation::BuildReactionForOrientation, HSReactionRelaxation.cpp:134-164). */
 int msgpu_set_reaction_scalar(msgpu_ctx *ctx, double kappa);

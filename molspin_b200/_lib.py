@@ -75,6 +75,8 @@ def _load() -> C.CDLL:
         "msgpu_device_bytes": (C.c_size_t, [P]),
         "msgpu_set_stream": (I, [P, P]),
         "msgpu_upload_hamiltonian_csr": (I, [P, I, pI, pI, pD]),
+        "msgpu_upload_hamiltonian_terms": (I, [P, I, pI, pI, I, pD, pD]),
+        "msgpu_set_hamiltonian_coefficients": (I, [P, pD]),
         "msgpu_set_reaction_scalar": (I, [P, D]),
         "msgpu_upload_reaction_csr": (I, [P, pI, pI, pD]),
         "msgpu_set_electron_pair": (I, [P, I, I]),

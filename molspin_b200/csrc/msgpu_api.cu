@@ -45,6 +45,13 @@ struct msgpu_ctx {
     // quartet-block form of H for the current electron strides
     DevBuf qrow, qcolt, qval, qbase;
     int q_s1 = 0, q_s2 = 0, q_D = 0, q_nblocks = 0;
+    // H as a fixed-pattern linear combination of terms (msgpu_upload_hamiltonian_terms):
+    // the host copy h_val then holds a generic combination (structure only)
+    bool terms = false;
+    int nterms = 0;
+    DevBuf hterms, qsrc;   // nterms x nnz complex128; CSR index of every quartet value slot (-1: zero)
+    size_t q_nslots = 0;
+    std::array<double, 16> hcoef{};  // current coefficients
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
     int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
     // resident (one warp per trajectory, whole time loop per launch) form
@@ -249,7 +256,7 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
                      &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d,
-                     &c->dense_part};
+                     &c->dense_part, &c->hterms, &c->qsrc};
     for (DevBuf *b : all) release(c, *b);
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
     for (auto &a : c->dense_allocs) cudaFree(a.first);
@@ -335,6 +342,8 @@ int msgpu_upload_hamiltonian_csr(msgpu_ctx *c, int dim, const int *rowptr, const
     c->h_col.assign(col, col + nnz);
     c->h_val.assign(val, val + 2 * static_cast<size_t>(nnz));
     c->q_D = 0;  // quartet form must be rebuilt
+    c->terms = false;
+    c->dense.have_u = false;  // a cached dense propagator belongs to the old H
     return MSGPU_OK;
 }
 
@@ -450,6 +459,49 @@ int msgpu_set_st_noise(msgpu_ctx *c, double st_rate, int mode, unsigned long lon
 }
 
 }  // extern "C"
+
+namespace msgpu {
+namespace {  // internal linkage, beside the other kernels
+
+// H = sum_k coef_k H_k on the common CSR pattern: complex128 values and
+// their FP32 hi/lo split; bit 2 of status on a non-finite value.
+struct TermCoef {
+    double c[16];
+};
+
+__global__ void k_combine_terms(const double2 *__restrict__ terms, int nterms, TermCoef cf, int nnz,
+                                double2 *__restrict__ val, float2 *__restrict__ hi, float2 *__restrict__ lo,
+                                int *__restrict__ status)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    double2 v = make_double2(0.0, 0.0);
+    for (int t = 0; t < nterms; ++t) {
+        const double2 x = terms[static_cast<size_t>(t) * nnz + k];
+        v.x += cf.c[t] * x.x;
+        v.y += cf.c[t] * x.y;
+    }
+    if (!isfinite(v.x) || !isfinite(v.y)) atomicOr(status, 2);
+    val[k] = v;
+    const float2 h = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    hi[k] = h;
+    lo[k] = make_float2(static_cast<float>(v.x - static_cast<double>(h.x)),
+                        static_cast<float>(v.y - static_cast<double>(h.y)));
+}
+
+// quartet value slot s (two FP32 per complex value) <- the CSR value it came from
+__global__ void k_quartet_refresh(const int *__restrict__ src, size_t nslots, const double2 *__restrict__ val,
+                                  float2 *__restrict__ qval)
+{
+    const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int k = src[s];
+    const double2 v = k >= 0 ? val[k] : make_double2(0.0, 0.0);
+    qval[s] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+}
+
+}  // namespace
+}  // namespace msgpu
 
 namespace {
 
@@ -842,6 +894,16 @@ int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
 }
 
 // Quartet-block form of H for the current electron strides (see QuartetC).
+int refresh_quartet_values(msgpu_ctx *c)
+{
+    if (!c->q_nslots) return MSGPU_OK;
+    k_quartet_refresh<<<static_cast<unsigned>((c->q_nslots + 255) / 256), 256, 0, c->stream>>>(
+        static_cast<const int *>(c->qsrc.p), c->q_nslots, static_cast<const double2 *>(c->hval.p),
+        static_cast<float2 *>(c->qval.p));
+    const cudaError_t e = cudaGetLastError();
+    return e ? cuda_fail(c, e, "quartet value refresh") : MSGPU_OK;
+}
+
 int build_quartet(msgpu_ctx *c)
 {
     if (c->q_D == c->D && c->q_s1 == c->s1 && c->q_s2 == c->s2) return MSGPU_OK;
@@ -851,11 +913,14 @@ int build_quartet(msgpu_ctx *c)
     std::vector<int2> blks;
     std::vector<float> vals;
     std::vector<std::pair<int, std::array<double, 32>>> blocks;  // (neighbour base, 16 complex)
+    std::vector<std::array<int, 16>> bsrc;                        // CSR index of each block entry
+    std::vector<int> src;                                         // CSR index per stored value slot
     for (int q = 0; q < Q; ++q) {
         const int lo = q % s2, mid = (q / s2) % (s1 / (2 * s2)), hi = q / (s1 / 2);
         const int b = hi * (2 * s1) + mid * (2 * s2) + lo;
         base[q] = b;
         blocks.clear();
+        bsrc.clear();
         for (int a = 0; a < 4; ++a) {
             const int r = b + off[a];
             for (int k = c->h_rowptr[r]; k < c->h_rowptr[r + 1]; ++k) {
@@ -868,13 +933,20 @@ int build_quartet(msgpu_ctx *c)
                     std::array<double, 32> z;
                     z.fill(0.0);
                     blocks.push_back({cb, z});
+                    std::array<int, 16> none;
+                    none.fill(-1);
+                    bsrc.push_back(none);
                 }
+                bsrc[slot][a * 4 + bi] = k;
                 blocks[slot].second[2 * (a * 4 + bi)] += c->h_val[2 * static_cast<size_t>(k)];
                 blocks[slot].second[2 * (a * 4 + bi) + 1] += c->h_val[2 * static_cast<size_t>(k) + 1];
             }
         }
-        std::sort(blocks.begin(), blocks.end(), [](auto &x, auto &y) { return x.first < y.first; });
-        for (auto &blk : blocks) {
+        std::vector<size_t> ord(blocks.size());
+        for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return blocks[x].first < blocks[y].first; });
+        for (size_t oi : ord) {
+            const auto &blk = blocks[oi];
             const auto &B = blk.second;  // 16 complex, row-major in the pair index
             auto re = [&](int a, int b) { return B[2 * (a * 4 + b)]; };
             auto im = [&](int a, int b) { return B[2 * (a * 4 + b) + 1]; };
@@ -919,6 +991,7 @@ int build_quartet(msgpu_ctx *c)
             for (auto &ab : order) {
                 vals.push_back(static_cast<float>(re(ab.first, ab.second)));
                 vals.push_back(static_cast<float>(im(ab.first, ab.second)));
+                src.push_back(bsrc[oi][ab.first * 4 + ab.second]);
             }
         }
         rowptr[q + 1] = static_cast<int>(blks.size());
@@ -942,6 +1015,16 @@ int build_quartet(msgpu_ctx *c)
     c->q_s2 = s2;
     c->q_nblocks = nb;
     c->q_tile = 0;
+    c->q_nslots = src.size();
+    if (c->terms) {
+        // the structure came from a generic combination of the terms; the
+        // values of the current coefficients come from the device CSR
+        if ((rc = ensure(c, c->qsrc, sizeof(int) * std::max<size_t>(1, src.size()), "quartet value map")))
+            return rc;
+        if ((e = cudaMemcpyAsync(c->qsrc.p, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, c->stream)))
+            return cuda_fail(c, e, "quartet value map");
+        if ((rc = refresh_quartet_values(c))) return rc;
+    }
     return MSGPU_OK;
 }
 
@@ -1012,6 +1095,69 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
 }  // namespace
 
 extern "C" {
+
+int msgpu_upload_hamiltonian_terms(msgpu_ctx *c, int dim, const int *rowptr, const int *col, int nterms,
+                                   const double *vals, const double *coef)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (nterms < 1 || nterms > 16 || !vals || !coef || dim < 4 || !rowptr)
+        return fail(c, MSGPU_ERR_INVALID, "Hamiltonian terms: 1..16 terms, values and coefficients required");
+    const int nnz = rowptr[dim];
+    if (nnz < 0) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian terms: malformed row pointer");
+    for (size_t i = 0; i < 2 * static_cast<size_t>(nnz) * nterms; ++i)
+        if (!std::isfinite(vals[i])) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian terms: non-finite value");
+    // a generic combination (fixed irrational-looking weights) fixes the
+    // sparsity and block structure for every combination of the terms
+    std::vector<double> gen(2 * static_cast<size_t>(nnz), 0.0);
+    for (int t = 0; t < nterms; ++t) {
+        const double w = 1.0 + 0.7548776662466927 * (t + 1) - std::floor(0.7548776662466927 * (t + 1));
+        for (size_t i = 0; i < gen.size(); ++i) gen[i] += w * vals[static_cast<size_t>(t) * gen.size() + i];
+    }
+    if (int rc = msgpu_upload_hamiltonian_csr(c, dim, rowptr, col, gen.data())) return rc;
+    int rc;
+    if ((rc = ensure(c, c->hterms, sizeof(double2) * std::max<size_t>(1, static_cast<size_t>(nnz) * nterms),
+                     "Hamiltonian terms")))
+        return rc;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->hterms.p, vals, sizeof(double2) * static_cast<size_t>(nnz) * nterms,
+                             cudaMemcpyHostToDevice, c->stream)))
+        return cuda_fail(c, e, "Hamiltonian terms upload");
+    c->terms = true;
+    c->nterms = nterms;
+    return msgpu_set_hamiltonian_coefficients(c, coef);
+}
+
+int msgpu_set_hamiltonian_coefficients(msgpu_ctx *c, const double *coef)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (!c->terms) return fail(c, MSGPU_ERR_STATE, "Hamiltonian coefficients: no terms uploaded");
+    if (!coef) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian coefficients: null array");
+    if (int rc = device_guard(c)) return rc;
+    TermCoef cf;
+    std::memset(&cf, 0, sizeof(cf));
+    for (int t = 0; t < c->nterms; ++t) {
+        if (!std::isfinite(coef[t])) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian coefficients: non-finite value");
+        cf.c[t] = coef[t];
+        c->hcoef[t] = coef[t];
+    }
+    if (int rc = ensure(c, c->status, sizeof(int), "status")) return rc;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream))) return cuda_fail(c, e, "Hamiltonian update");
+    k_combine_terms<<<ceil_div(std::max(1, c->nnz), 256), 256, 0, c->stream>>>(
+        static_cast<const double2 *>(c->hterms.p), c->nterms, cf, c->nnz, static_cast<double2 *>(c->hval.p),
+        static_cast<float2 *>(c->hhi.p), static_cast<float2 *>(c->hlo.p), static_cast<int *>(c->status.p));
+    if ((e = cudaGetLastError())) return cuda_fail(c, e, "Hamiltonian update");
+    // the quartet form keeps its structure; only its values follow H
+    if (c->q_D == c->D)
+        if (int rc = refresh_quartet_values(c)) return rc;
+    c->dense.have_u = false;
+    int status = 0;
+    if ((e = cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "Hamiltonian update");
+    if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian coefficients: non-finite combined value");
+    return MSGPU_OK;
+}
 
 int msgpu_upload_factors(msgpu_ctx *c, int dim, int ntraj, const double *factors)
 {

@@ -111,6 +111,22 @@ class HSPropagatorB200:
         _check(self.ctx, L.lib.msgpu_upload_hamiltonian_csr(self.ctx, D, L.iptr(rowptr), L.iptr(col), L.dptr(v)))
         self.D = D
 
+    def set_hamiltonian_terms(self, rowptr, col, vals, coef):
+        """H = sum_k coef_k H_k on one CSR pattern (vals: nterms x nnz complex);
+        later field changes go through set_hamiltonian_coefficients."""
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        v = np.ascontiguousarray(np.asarray(vals, dtype=np.complex128))
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        D = len(rowptr) - 1
+        _check(self.ctx, L.lib.msgpu_upload_hamiltonian_terms(self.ctx, D, L.iptr(rowptr), L.iptr(col), v.shape[0],
+                                                              L.dptr(v.view(np.float64).reshape(-1)), L.dptr(c)))
+        self.D = D
+
+    def set_hamiltonian_coefficients(self, coef):
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        _check(self.ctx, L.lib.msgpu_set_hamiltonian_coefficients(self.ctx, L.dptr(c)))
+
     def set_reaction(self, kappa: float | None = None, csr=None):
         if csr is None:
             _check(self.ctx, L.lib.msgpu_set_reaction_scalar(self.ctx, float(kappa)))

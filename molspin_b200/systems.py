@@ -126,6 +126,33 @@ def _zeeman(sys_: SpinSystem, field_T: np.ndarray, g: float = G_ELECTRON):
         sys_.linear.append((e, COMMON_PREFACTOR * g * np.asarray(field_T, dtype=np.float64)))
 
 
+def field_terms(system: SpinSystem):
+    """H(B) = H_0 + Bx Z_x + By Z_y + Bz Z_z (B in T) on one CSR pattern.
+
+    H_0 is the system without its linear (Zeeman) terms, Z_a the electron
+    Zeeman operator of a 1 T field along axis a (g = 2.0023, as radical_pair
+    builds it).  Returns (rowptr, col, vals) with vals of shape (4, nnz):
+    the input of msgpu_upload_hamiltonian_terms, whose coefficients are then
+    (1, Bx, By, Bz).  Each term stores explicit zeros where the others have
+    entries, so every field direction shares the pattern."""
+    import scipy.sparse as sp
+    base = SpinSystem(mult=list(system.mult), names=list(system.names), electrons=system.electrons,
+                      bilinear=list(system.bilinear))
+    mats = []
+    for sysk in [base] + [None] * 3:
+        if sysk is None:
+            sysk = SpinSystem(mult=list(system.mult), names=list(system.names), electrons=system.electrons)
+            _zeeman(sysk, np.eye(3)[len(mats) - 1])
+        r, c, v = sysk.hamiltonian_csr()
+        D = len(r) - 1
+        mats.append(sp.csr_matrix((v, c, r), shape=(D, D)))
+    pattern = sum(abs(m) for m in mats).tocsr()
+    pattern.sort_indices()
+    rows = np.repeat(np.arange(pattern.shape[0]), np.diff(pattern.indptr))
+    vals = np.stack([np.asarray(m[rows, pattern.indices]).ravel() for m in mats]).astype(np.complex128)
+    return pattern.indptr.astype(np.int32), pattern.indices.astype(np.int32), vals
+
+
 def _hyperfine(sys_: SpinSystem, e: int, n: int, A_mT: np.ndarray, g: float = G_ELECTRON):
     sys_.bilinear.append((e, n, COMMON_PREFACTOR * 1e-3 * g * np.asarray(A_mT, dtype=np.float64)))
 

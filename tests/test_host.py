@@ -103,3 +103,27 @@ def test_plan_validation():
     p.validate()
     assert p.krylovsize == 16
     assert abs(hs.yield_correction(0.5, 0.02) - orc.yield_correction(0.5, 0.02)) < 1e-15
+
+
+def test_field_terms_reproduce_the_hamiltonian():
+    # H_0 + Bx Zx + By Zy + Bz Zz on the union pattern equals H(B) built directly
+    rng = np.random.default_rng(21)
+    ta = [S._aniso_tensor(rng, 1.5) for _ in range(2)]
+    tb = [S._aniso_tensor(rng, 1.5)]
+    B = np.array([12e-6, -30e-6, 41e-6])
+    direct = S.radical_pair([2, 2], [2], ta, tb, B, sink_rate=1e-3)
+    r, c, v = S.field_terms(direct)
+    coef = np.array([1.0, *B])
+    D = direct.dim
+    combined = np.zeros((D, D), dtype=np.complex128)
+    for k in range(4):
+        for row in range(D):
+            for idx in range(r[row], r[row + 1]):
+                combined[row, c[idx]] += coef[k] * v[k, idx]
+    rd, cd, vd = direct.hamiltonian_csr()
+    ref = np.zeros((D, D), dtype=np.complex128)
+    for row in range(D):
+        for idx in range(rd[row], rd[row + 1]):
+            ref[row, cd[idx]] += vd[idx]
+    assert np.max(np.abs(combined - ref)) < 1e-12 * np.max(np.abs(ref))
+    assert v.shape == (4, r[-1])
