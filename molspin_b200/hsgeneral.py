@@ -279,3 +279,49 @@ def run_stochastic_yields(system: SpinSystem, plan: HSExecutionPlan, device: int
         ens = ens * c
         per = per * c
     return {"names": [n for n, _, _ in obs], "yields": ens, "traj_yields": per, "values": values, "times": times}
+
+
+def run_powder_yields(system: SpinSystem, plan: HSExecutionPlan, field_T: float, directions: np.ndarray,
+                      weights: np.ndarray | None = None, device: int = 0, factors: np.ndarray | None = None,
+                      hbm_budget: int = 0) -> dict:
+    """The orientation loop of TaskHSGeneral::RunLocal (TaskHSGeneral.cpp:347-575)
+    for a field of strength field_T (T) along each unit vector of `directions`.
+
+    One device context holds H as fixed-pattern terms (H_0 + Bx Zx + By Zy +
+    Bz Zz, systems.field_terms); each orientation only changes the field
+    coefficients on the device.  Every orientation starts from the same
+    trace samples (a copy of the prepared factors, TaskHSGeneral.cpp:359) and
+    draws its own noise stream; the ensemble yields are averaged with the
+    weights (uniform when omitted), TaskHSGeneral.cpp:568-575.  The system's
+    own Zeeman terms are replaced by the orientation's field."""
+    plan.validate()
+    dirs = np.asarray(directions, dtype=np.float64).reshape(-1, 3)
+    w = np.full(len(dirs), 1.0 / len(dirs)) if weights is None else np.asarray(weights, dtype=np.float64)
+    times = time_grid(plan.totaltime, plan.timestep)
+    M = plan.montecarlosamples
+    if factors is None:
+        factors = system.trace_samples(M, plan.seed)
+    from .systems import field_terms
+    rowptr, col, vals = field_terms(system)
+    obs = system.observables()
+    per_orientation = []
+    with HSPropagatorB200(device, hbm_budget) as prop:
+        prop.set_hamiltonian_terms(rowptr, col, vals, [1.0, *(field_T * dirs[0])])
+        prop.set_reaction(kappa=system.kappa())
+        prop.set_electron_pair(*system.electron_strides())
+        prop.set_observables([(op, rate) for _, op, rate in obs])
+        for i, d in enumerate(dirs):
+            prop.set_hamiltonian_coefficients([1.0, *(field_T * d)])
+            if system.st_rate > 0.0:
+                if plan.noise == "reference":
+                    bits = reference_flip_bits(plan.seed, system.st_rate, times, M, i)
+                    prop.set_noise(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M)
+                else:
+                    prop.set_noise(system.st_rate, L.NOISE_PHILOX, int(plan.seed) * 1_000_003 + i)
+            prop.set_factors(factors)
+            prop.propagate(times, plan.krylovsize, plan.gpuprecision)
+            per_orientation.append(prop.yields()[1])
+    ens = np.asarray(per_orientation)
+    if plan.yieldcorrections:
+        ens = ens * yield_correction(plan.totaltime, max(rate for _, _, rate in obs))
+    return {"names": [n for n, _, _ in obs], "yields": w @ ens, "orientation_yields": ens, "weights": w}
