@@ -59,6 +59,14 @@ extern "C" {
  * accumulation).  Precision must be MSGPU_PREC_BF16X3 (two-part split, three
  * products) or MSGPU_PREC_BF16X6 (three-part split, six products). */
 #define MSGPU_PROP_DENSE 1
+/* propagationmethod=autoexpm (HSPropagator.cpp:58-62 -> SpinSpace::HighamProp,
+ * SpinSpace_operators.cpp:1028-1134): truncated Taylor series of
+ * exp(dt(G - mu I)), G = -iH - K, mu = trace(G)/D, on s sub-steps with
+ * s = ceil(dt ||G - mu I||_1 / 4) and the a-priori degree for the tolerance
+ * MSGPU_OPT_TAYLOR_TOL; complex128 only, any K.  The reference picks (m, s)
+ * from a random norm estimate; this choice is deterministic and no less
+ * accurate. */
+#define MSGPU_PROP_TAYLOR 2
 #define MSGPU_PREC_BF16X3 2
 #define MSGPU_PREC_BF16X6 3
 
@@ -66,6 +74,8 @@ extern "C" {
 #define MSGPU_OPT_DENSE_RENORMALIZE 1 /* 1 (default): the dense form restores the exact
                                         Haberkorn survival |psi|^2 e^{-2 kappa t} of each
                                         trajectory every step (scalar K only); 0: off */
+#define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
+                                        (default, "double"), 2^-24 ("single"), 2^-10 ("half") */
 
 /* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
  * dimensions (the whole time loop in one launch, one warp per trajectory,

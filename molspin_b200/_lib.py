@@ -30,6 +30,8 @@ REC_ARNOLDI = 1
 REC_LANCZOS = 2
 PROP_KRYLOV = 0
 PROP_DENSE = 1
+PROP_TAYLOR = 2
+OPT_TAYLOR_TOL = 2
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
 OPT_DENSE_RENORMALIZE = 1

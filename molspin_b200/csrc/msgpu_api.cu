@@ -64,6 +64,9 @@ struct msgpu_ctx {
     // reaction
     bool k_scalar = true;
     double kappa = 0.0;
+    double2 k_trace = {0.0, 0.0};  // trace of a CSR K
+    double k_norm1 = 0.0;          // its 1-norm (max column sum)
+    double taylor_tol = 0x1p-53;   // MSGPU_OPT_TAYLOR_TOL
     DevBuf krow, kcol, kval;
     // electron pair
     int s1 = 0, s2 = 0;
@@ -277,6 +280,11 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
         c->dense_renorm = value != 0.0;
         return MSGPU_OK;
     }
+    if (key == MSGPU_OPT_TAYLOR_TOL) {
+        if (!(value > 0.0 && value < 1.0)) return fail(c, MSGPU_ERR_INVALID, "Taylor tolerance must be in (0, 1)");
+        c->taylor_tol = value;
+        return MSGPU_OK;
+    }
     return fail(c, MSGPU_ERR_INVALID, "unknown option");
 }
 
@@ -383,6 +391,18 @@ int msgpu_upload_reaction_csr(msgpu_ctx *c, const int *rowptr, const int *col, c
         (e = cudaStreamSynchronize(c->stream)))
         return cuda_fail(c, e, "reaction upload");
     c->k_scalar = false;
+    // trace and 1-norm (max column sum) for the Taylor propagator's shift and sub-steps
+    std::vector<double> colsum(D, 0.0);
+    c->k_trace = make_double2(0.0, 0.0);
+    for (int r = 0; r < D; ++r)
+        for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+            colsum[col[k]] += std::hypot(val[2 * k], val[2 * k + 1]);
+            if (col[k] == r) {
+                c->k_trace.x += val[2 * k];
+                c->k_trace.y += val[2 * k + 1];
+            }
+        }
+    c->k_norm1 = colsum.empty() ? 0.0 : *std::max_element(colsum.begin(), colsum.end());
     return MSGPU_OK;
 }
 
@@ -1218,11 +1238,15 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     }
     if (p->precision != MSGPU_PREC_C128 && p->precision != MSGPU_PREC_C64)
         return fail(c, MSGPU_ERR_INVALID, "run: unknown precision");
-    if (p->propagator != MSGPU_PROP_KRYLOV) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
-    if (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov)
+    const bool taylor = p->propagator == MSGPU_PROP_TAYLOR;
+    if (p->propagator != MSGPU_PROP_KRYLOV && !taylor) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
+    if (taylor && p->precision != MSGPU_PREC_C128)
+        return fail(c, MSGPU_ERR_INVALID, "run: the Taylor propagator is complex128 only");
+    if (!taylor && (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov))
         return fail(c, MSGPU_ERR_INVALID, "run: krylov_dim must be in 1..32");
     int rec = p->recurrence;
-    if (rec == MSGPU_REC_AUTO) rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
+    if (rec == MSGPU_REC_AUTO || taylor)
+        rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
     if (rec == MSGPU_REC_LANCZOS && !c->k_scalar)
         return fail(c, MSGPU_ERR_INVALID, "run: Lanczos requires a scalar reaction operator K");
     if (p->precision == MSGPU_PREC_C64 && rec != MSGPU_REC_LANCZOS)
@@ -1238,11 +1262,11 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     if (int rc = device_guard(c)) return rc;
 
     const int D = c->D, ldm = c->ldm, M = c->M;
-    const int m = std::min(p->krylov_dim, D);
+    const int m = taylor ? 1 : std::min(p->krylov_dim, D);  // the Taylor step needs no Krylov basis
     const int prec = p->precision;
-    if (resident_warps(c, prec, m) > 0) return run_resident(c, p, prec, m);
+    if (!taylor && resident_warps(c, prec, m) > 0) return run_resident(c, p, prec, m);
     if (c->form == MSGPU_FORM_RESIDENT)
-        return fail(c, MSGPU_ERR_INVALID, "run: the resident form does not fit this dimension / recurrence");
+        return fail(c, MSGPU_ERR_INVALID, "run: the resident form does not fit this dimension / recurrence / propagator");
     const int nobs = static_cast<int>(c->obs.size());
     const size_t n = static_cast<size_t>(D) * ldm;
     // The complex64 state lives in slot 0 of the Lanczos basis: park it in the
@@ -1328,12 +1352,61 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                                   static_cast<int>(expm_warps * expm_smem_warp))))
         return cuda_fail(c, e, "expm shared memory");
 
+    // Taylor propagator: the shift mu = trace(G)/D and a bound on ||G - mu I||_1
+    double2 tmu = make_double2(0.0, 0.0);
+    double tnorm = 0.0;
+    if (taylor) {
+        if (int rc = ensure(c, c->work_d, 4 * sizeof(double), "Taylor statistics")) return rc;
+        k_g_stats<<<1, 256, 0, st>>>(Hd, D, static_cast<double *>(c->work_d.p));
+        double hs[3] = {0.0, 0.0, 0.0};
+        if ((e = cudaMemcpyAsync(hs, c->work_d.p, sizeof(hs), cudaMemcpyDeviceToHost, st)) ||
+            (e = cudaStreamSynchronize(st)))
+            return cuda_fail(c, e, "Taylor statistics");
+        const double2 ktr = c->k_scalar ? make_double2(c->kappa * D, 0.0) : c->k_trace;
+        const double kn = c->k_scalar ? std::abs(c->kappa) : c->k_norm1;
+        // trace(G) = -i trace(H) - trace(K)
+        tmu = make_double2((hs[1] - ktr.x) / D, (-hs[0] - ktr.y) / D);
+        tnorm = hs[2] + kn + std::hypot(tmu.x, tmu.y);
+        if (!std::isfinite(tnorm)) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite Hamiltonian norm");
+    }
     for (int s = 0; s < steps; ++s) {
         c->prof_tick = s;
         const double dt = p->times[s + 1] - p->times[s];
         const long long g = g0 + s;
         if ((e = cudaMemsetAsync(c->mdim.p, 0, ldm * sizeof(int), st))) return cuda_fail(c, e, "mdim reset");
-        if (prec == MSGPU_PREC_C128) {
+        if (taylor) {
+            // exp(dt (G - mu I)) by s sub-steps of a degree-mt Taylor series
+            // (theta^(mt+1)/(mt+1)! e^theta <= tol with theta = |dt| ||G - mu I||_1 / s <= 4),
+            // each ending with F <- e^{dt mu / s} F (SpinSpace::HighamProp's loop)
+            double2 *F = static_cast<double2 *>(c->psi128.p);
+            double2 *cur = static_cast<double2 *>(c->wbuf.p), *nxt = static_cast<double2 *>(c->zbuf.p);
+            const int nsub = std::max(1, static_cast<int>(std::ceil(std::abs(dt) * tnorm / 4.0)));
+            const double theta = std::abs(dt) * tnorm / nsub;
+            int mt = 1;
+            for (double rem = theta * theta / 2.0; rem * std::exp(theta) > c->taylor_tol && mt < 55; ++mt)
+                rem *= theta / (mt + 2);
+            const double er = std::exp(dt * tmu.x / nsub), ea = dt * tmu.y / nsub;
+            const double2 eta = make_double2(er * std::cos(ea), er * std::sin(ea));
+            if ((e = cudaMemcpyAsync(cur, F, n * sizeof(double2), cudaMemcpyDeviceToDevice, st)))
+                return cuda_fail(c, e, "Taylor step");
+            dim3 tgrid(ceil_div(D, 8), ldm / 32), tblock(32, 8);
+            for (int sub = 0; sub < nsub; ++sub) {
+                for (int k = 1; k <= mt; ++k) {
+                    Timed tm(c, KC_APPLY);
+                    k_taylor_term<<<tgrid, tblock, 0, st>>>(Hd, Kd, kappa, tmu, cur, nxt, F, dt / (nsub * k), D, ldm);
+                    std::swap(cur, nxt);
+                }
+                Timed tm(c, KC_ORTH);
+                k_taylor_rescale<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(F, cur, eta, n);
+            }
+            {
+                Timed tm(c, KC_COMBINE);
+                k_combine<double2, false><<<qgrid, qblock, 0, st>>>(
+                    F, nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz, g, 1, pstep(s),
+                    s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, static_cast<double *>(c->qpart_obs.p),
+                    static_cast<double *>(c->qpart_nrm.p));
+            }
+        } else if (prec == MSGPU_PREC_C128) {
             double2 *V = static_cast<double2 *>(c->basis.p);
             double2 *bufA = static_cast<double2 *>(c->wbuf.p), *bufB = static_cast<double2 *>(c->zbuf.p);
             double2 *dots = static_cast<double2 *>(c->part2.p);  // [3][m+1][ldm]: h1, h2, norm

@@ -500,6 +500,87 @@ __global__ void k_krylov_expm(const double2 *__restrict__ hess, const double *__
     if (!ok && lane == 0 && t < M) atomicOr(status, 1);
 }
 
+// ---------------------------------------------------------------- Taylor propagator
+// One term of the truncated Taylor series of exp(tau (G - mu I)) applied to
+// the trajectory block (HSPropagator's autoexpm, SpinSpace::HighamProp,
+// SpinSpace_operators.cpp:1028-1134): out = scale (G - mu I) in with
+// G = -iH - K, scale = tau / (s k), and F += out.  Thread (row, trajectory);
+// a warp covers 32 trajectories of one row (coalesced 16-byte accesses).
+__global__ void __launch_bounds__(256)
+k_taylor_term(CsrD H, CsrD K, double kappa, double2 mu, const double2 *__restrict__ in, double2 *__restrict__ out,
+              double2 *__restrict__ F, double scale, int D, int ldm)
+{
+    const int t = blockIdx.y * 32 + threadIdx.x;
+    const int r = blockIdx.x * 8 + threadIdx.y;
+    if (r >= D) return;
+    double2 h = make_double2(0.0, 0.0);
+    for (int k = __ldg(H.rowptr + r); k < __ldg(H.rowptr + r + 1); ++k)
+        h = cfma(H.val[k], in[static_cast<size_t>(__ldg(H.col + k)) * ldm + t], h);
+    const size_t e = static_cast<size_t>(r) * ldm + t;
+    const double2 x = in[e];
+    double2 g = make_double2(h.y, -h.x);  // -i (H x)_r
+    if (K.rowptr) {
+        double2 kk = make_double2(0.0, 0.0);
+        for (int k = __ldg(K.rowptr + r); k < __ldg(K.rowptr + r + 1); ++k)
+            kk = cfma(K.val[k], in[static_cast<size_t>(__ldg(K.col + k)) * ldm + t], kk);
+        g = csub(g, kk);
+    } else {
+        g = csub(g, cscale(x, kappa));
+    }
+    g = csub(g, cmul(mu, x));
+    const double2 o = cscale(g, scale);
+    out[e] = o;
+    const double2 f = F[e];
+    F[e] = make_double2(f.x + o.x, f.y + o.y);
+}
+
+// End of a Taylor sub-step: F <- eta F (the shift e^{tau mu / s}), B <- F.
+__global__ void k_taylor_rescale(double2 *__restrict__ F, double2 *__restrict__ B, double2 eta, size_t n)
+{
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 f = cmul(eta, F[i]);
+    F[i] = f;
+    B[i] = f;
+}
+
+// trace(H) and max_r sum_k |H_rk| (= the 1-norm of a Hermitian H) in a fixed
+// order: one block; out = {tr.re, tr.im, max row sum}.
+__global__ void __launch_bounds__(256) k_g_stats(CsrD H, int D, double *__restrict__ out)
+{
+    __shared__ double sre[256], sim[256], smx[256];
+    double tr = 0.0, ti = 0.0, mx = 0.0;
+    for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        double rs = 0.0;
+        for (int k = H.rowptr[r]; k < H.rowptr[r + 1]; ++k) {
+            const double2 v = H.val[k];
+            rs += sqrt(v.x * v.x + v.y * v.y);
+            if (H.col[k] == r) {
+                tr += v.x;
+                ti += v.y;
+            }
+        }
+        mx = fmax(mx, rs);
+    }
+    sre[threadIdx.x] = tr;
+    sim[threadIdx.x] = ti;
+    smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (static_cast<int>(threadIdx.x) < w) {
+            sre[threadIdx.x] += sre[threadIdx.x + w];
+            sim[threadIdx.x] += sim[threadIdx.x + w];
+            smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sre[0];
+        out[1] = sim[0];
+        out[2] = smx[0];
+    }
+}
+
 // Krylov exponential of the Lanczos form (tridiagonal, see
 // warp_tridiag_expm_e1): one warp per trajectory.  Coefficients as in
 // k_krylov_expm: coef[j][t] = beta0 * vscale_j * y_j.
