@@ -42,6 +42,20 @@ long long msgpu_host_build_hamiltonian(int nspins, const int *mult, int nlin, co
  * fixed (leading) state; returns 0 on success. */
 int msgpu_host_trace_samples(double seed, const double *fixed, int F, int Z, int M, double *out);
 
+
+/* The reference flip stream for several dephasing Operators on the same
+ * electron pair (st_rates: each Operator's rate; event rate = rate / 2):
+ * ApplyStochasticRelaxationHilbert's superposed-Poisson branch
+ * (SpinSpace_relaxation.cpp:1239-1252) -- per half step and trajectory one
+ * Poisson count of mean (sum of event rates) h and one discrete channel draw
+ * per event, from the same generator as msgpu_host_reference_flip_bits.
+ * Every channel applies P_S - P_T, so the bit is the parity of the count;
+ * replay it with MSGPU_NOISE_REPLAY and st_rate = the sum of the rates.  One
+ * rate reduces to msgpu_host_reference_flip_bits.  Returns 0 on success. */
+int msgpu_host_reference_flip_bits_multi(double seed, int seed_mode, unsigned long long orientation,
+                                         const double *st_rates, int nterms, const double *times, int ntimes, int M,
+                                         unsigned char *bits);
+
 /* bits: ((ntimes-1)*2*M + 7)/8 bytes.  seed_mode 0: stream of orientation
  * `orientation` derived from the task seed; 1: std::mt19937(seed) directly. */
 int msgpu_host_reference_flip_bits(double seed, int seed_mode, unsigned long long orientation, double st_rate,

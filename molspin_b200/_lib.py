@@ -109,6 +109,7 @@ def _load() -> C.CDLL:
         "msgpu_host_build_hamiltonian": (C.c_longlong, [I, pI, I, pI, pD, I, pI, pI, pD, pI, pI, pD]),
         "msgpu_host_trace_samples": (I, [D, pD, I, I, I, pD]),
         "msgpu_host_reference_flip_bits": (I, [D, I, C.c_ulonglong, D, pD, I, I, pU8]),
+        "msgpu_host_reference_flip_bits_multi": (I, [D, I, C.c_ulonglong, pD, I, pD, I, I, pU8]),
         "msgpu_host_philox_flip_bits": (I, [C.c_ulonglong, C.c_uint, C.c_longlong, D, pD, I, I, pU8]),
         "msgpu_host_time_grid": (C.c_long, [D, D, pD, C.c_long]),
     }

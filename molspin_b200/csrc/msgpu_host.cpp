@@ -256,6 +256,54 @@ int msgpu_host_reference_flip_bits(double seed, int seed_mode, unsigned long lon
     return 0;
 }
 
+int msgpu_host_reference_flip_bits_multi(double seed, int seed_mode, unsigned long long orientation,
+                                         const double *st_rates, int nterms, const double *times, int ntimes, int M,
+                                         unsigned char *bits)
+{
+    if (nterms < 1 || !st_rates || ntimes < 1 || M <= 0 || !bits) return 1;
+    if (nterms == 1) return msgpu_host_reference_flip_bits(seed, seed_mode, orientation, st_rates[0], times, ntimes, M, bits);
+    std::vector<double> rates(nterms);
+    double total = 0.0;
+    for (int k = 0; k < nterms; ++k) {
+        if (!(st_rates[k] > 0.0) || !std::isfinite(st_rates[k])) return 1;
+        rates[k] = 0.5 * st_rates[k];  // event rate of a dephasing Operator: rate / 2
+        total += rates[k];
+    }
+    std::mt19937 g;
+    if (seed_mode == 0) {
+        const double s = seed == 0.0 ? 1.0 : seed;
+        std::mt19937 source;
+        source.seed(static_cast<std::mt19937::result_type>(s));
+        std::vector<std::mt19937::result_type> sd{0x5354524cU, 0x554e4954U,
+            static_cast<std::mt19937::result_type>(orientation & 0xffffffffULL),
+            static_cast<std::mt19937::result_type>(orientation >> 32)};
+        for (unsigned i = 0; i < 8; ++i) sd.push_back(source());
+        std::seed_seq seq(sd.begin(), sd.end());
+        g = std::mt19937(seq);
+    } else {
+        g = std::mt19937(static_cast<std::mt19937::result_type>(seed));
+    }
+    const long long steps = ntimes - 1;
+    std::memset(bits, 0, static_cast<size_t>((steps * 2 * M + 7) / 8));
+    for (long long s = 0; s < steps; ++s) {
+        const double h = 0.5 * (times[s + 1] - times[s]);
+        if (h == 0.0) continue;
+        for (int half = 0; half < 2; ++half) {
+            std::poisson_distribution<unsigned long long> count(total * h);
+            std::discrete_distribution<size_t> channel(rates.begin(), rates.end());
+            for (int c = 0; c < M; ++c) {
+                const unsigned long long events = count(g);
+                for (unsigned long long e = 0; e < events; ++e) (void)channel(g);
+                if (events & 1ULL) {
+                    const long long bit = (s * 2 + half) * M + c;
+                    bits[bit >> 3] |= static_cast<unsigned char>(1u << (bit & 7));
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 int msgpu_host_philox_flip_bits(unsigned long long seed, unsigned int traj_offset, long long step_offset,
                                 double st_rate, const double *times, int ntimes, int M, unsigned char *bits)
 {

@@ -214,6 +214,21 @@ class HSPropagatorB200:
         return ms.value, n.value
 
 
+def reference_flip_bits_multi(seed: float, st_rates, times: np.ndarray, M: int, orientation: int = 0,
+                              seed_mode: int = 0) -> np.ndarray:
+    """The reference's flip stream for several dephasing Operators on the same
+    electron pair (st_rates: each Operator's rate), as parity bits; replay with
+    st_rate = sum(st_rates)."""
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    r = np.ascontiguousarray(st_rates, dtype=np.float64)
+    bits = np.zeros(max(1, ((len(t) - 1) * 2 * M + 7) // 8), dtype=np.uint8)
+    rc = L.lib.msgpu_host_reference_flip_bits_multi(float(seed), int(seed_mode), int(orientation), L.dptr(r), len(r),
+                                                    L.dptr(t), len(t), int(M), L.u8ptr(bits))
+    if rc:
+        raise ValueError("flip stream generation failed")
+    return bits
+
+
 def reference_flip_bits(seed: float, st_rate: float, times: np.ndarray, M: int, orientation: int = 0,
                         seed_mode: int = 0) -> np.ndarray:
     """The reference's singlet-triplet flip stream for one orientation, as bits."""

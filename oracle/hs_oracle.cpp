@@ -522,6 +522,47 @@ int oracle_st_flip_bits(double seed, int seed_mode, unsigned long long orientati
     return 0;
 }
 
+// Several stochastic relaxation terms on the same electron pair (all with
+// U = P_S - P_T): the reference's superposed-Poisson branch
+// (ApplyStochasticRelaxationHilbert, SpinSpace_relaxation.cpp:1239-1252):
+// per half step and column one Poisson count of mean (sum of event rates) h,
+// then one discrete channel draw per event, in that order.  With every
+// channel applying the same involution the column is flipped when the count
+// is odd; bit layout as oracle_st_flip_bits.  One term reduces to
+// oracle_st_flip_bits (the Bernoulli branch).
+int oracle_st_flip_bits_multi(double seed, int seed_mode, unsigned long long orientation, const double *eventRates,
+                              int nterms, const double *times, int ntimes, int M, unsigned char *bits)
+{
+    if (nterms < 1 || !eventRates) return 1;
+    if (nterms == 1) return oracle_st_flip_bits(seed, seed_mode, orientation, eventRates[0], times, ntimes, M, bits);
+    std::mt19937 g = seed_mode == 0 ? relaxation_generator(seeded(seed), orientation)
+                                    : std::mt19937(static_cast<std::mt19937::result_type>(seed));
+    double total = 0.0;
+    for (int k = 0; k < nterms; ++k) {
+        if (!(eventRates[k] > 0.0) || !std::isfinite(eventRates[k])) return 1;
+        total += eventRates[k];
+    }
+    const int steps = ntimes - 1;
+    std::memset(bits, 0, (static_cast<size_t>(steps) * 2 * M + 7) / 8);
+    for (int s = 0; s < steps; ++s) {
+        const double h = 0.5 * (times[s + 1] - times[s]);
+        if (h == 0.0) continue;  // no RNG consumption
+        for (int half = 0; half < 2; ++half) {
+            std::poisson_distribution<unsigned long long> count(total * h);
+            std::discrete_distribution<size_t> channel(eventRates, eventRates + nterms);
+            for (int c = 0; c < M; ++c) {
+                const unsigned long long events = count(g);
+                for (unsigned long long e = 0; e < events; ++e) (void)channel(g);
+                if (events & 1ULL) {
+                    const size_t bit = (static_cast<size_t>(s) * 2 + half) * M + c;
+                    bits[bit >> 3] |= static_cast<unsigned char>(1u << (bit & 7));
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 // One ApplyStochasticRelaxationHilbert call on D x M factors (in place), with
 // a std::mt19937(seed) generator; U given as CSR.  Used by the analytic-law pins.
 int oracle_apply_st(int D, const int *urow, const int *ucol, const double *uval, double eventRate,

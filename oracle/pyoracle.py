@@ -32,6 +32,7 @@ def lib():
             "oracle_st_unitary": (C.c_long, [I, pI, I, I, pI, pI, pD]),
             "oracle_trace_samples": (I, [D, pD, I, I, I, pD]),
             "oracle_st_flip_bits": (I, [D, I, C.c_ulonglong, D, pD, I, I, pU8]),
+            "oracle_st_flip_bits_multi": (I, [D, I, C.c_ulonglong, pD, I, pD, I, I, pU8]),
             "oracle_apply_st": (I, [I, pI, pI, pD, D, D, C.c_uint, I, pD]),
             "oracle_hs_stochastic": (I, [I, I, pI, pI, pD, pI, pI, pD, D, pD, pD, I, I, I, pI, pI, pD, D, I, D, I,
                                          C.c_ulonglong, pU8, I, pI, pL, pI, pD, pD, pD, pD, pD, I]),
@@ -106,6 +107,18 @@ def st_flip_bits(seed: float, seed_mode: int, orientation: int, event_rate: floa
     bits = np.zeros(max(1, ((len(t) - 1) * 2 * M + 7) // 8), np.uint8)
     lib().oracle_st_flip_bits(seed, seed_mode, orientation, event_rate, _p(t, C.c_double), len(t), M,
                               _p(bits, C.c_ubyte))
+    return bits
+
+
+def st_flip_bits_multi(seed: float, seed_mode: int, orientation: int, event_rates, times, M: int) -> np.ndarray:
+    """Flip bits of several dephasing terms on one electron pair (superposed-Poisson branch)."""
+    t = np.ascontiguousarray(times, np.float64)
+    r = np.ascontiguousarray(event_rates, np.float64)
+    bits = np.zeros(max(1, ((len(t) - 1) * 2 * M + 7) // 8), np.uint8)
+    rc = lib().oracle_st_flip_bits_multi(seed, seed_mode, orientation, _p(r, C.c_double), len(r), _p(t, C.c_double),
+                                         len(t), M, _p(bits, C.c_ubyte))
+    if rc:
+        raise ValueError("oracle flip stream failed")
     return bits
 
 

@@ -230,3 +230,18 @@ def test_error_paths():
             p.set_hamiltonian(r, c, v)
             p.set_factors(system.trace_samples(64, 1.0))
         assert e.value.code == L.MSGPU_ERR_BUDGET
+
+
+def test_multi_term_dephasing_stream_replayed():
+    # two dephasing Operators on the pair: the reference's superposed-Poisson
+    # stream as parity bits, replayed on the device against the oracle
+    system = h.random_system([2, 3], [2, 2], seed=12, st_rate=0.0, hf_scale=3.0)
+    rates = [0.05, 0.08]
+    system.st_rate = sum(rates)
+    M, times = 40, S.time_grid(40.0, 1.0)
+    F = system.trace_samples(M, 3.0)
+    bits = hs.reference_flip_bits_multi(9.0, rates, times, M, 1)
+    assert bits.any()
+    per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
+    ref = _oracle(system, F, times, 16, U=True, kappa=system.kappa(), noise_mode=1, flip_bits=bits)
+    assert _rel(per, ref["traj_yield"]) < 1e-10

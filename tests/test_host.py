@@ -127,3 +127,21 @@ def test_field_terms_reproduce_the_hamiltonian():
             ref[row, cd[idx]] += vd[idx]
     assert np.max(np.abs(combined - ref)) < 1e-12 * np.max(np.abs(ref))
     assert v.shape == (4, r[-1])
+
+
+def test_multi_term_flip_stream_matches_oracle_and_law():
+    # several dephasing Operators on one pair: superposed Poisson counts with
+    # channel marks, parity bits; bitwise equal to the oracle, reduces to the
+    # Bernoulli stream for one term, and flips with p = (1 - exp(-2 L h)) / 2
+    times = S.time_grid(40.0, 1.0)
+    M = 300
+    for rates, seed, orient in (([0.3, 0.5], 7.0, 0), ([0.1, 0.2, 0.05], 2.0, 5)):
+        host = hs.reference_flip_bits_multi(seed, rates, times, M, orient)
+        ref = orc.st_flip_bits_multi(seed, 0, orient, [0.5 * r for r in rates], times, M)
+        np.testing.assert_array_equal(host, ref)
+        total = 0.5 * sum(rates)
+        p = -0.5 * np.expm1(-2.0 * total * 0.5)
+        frac = np.unpackbits(host, bitorder="little")[: (len(times) - 1) * 2 * M].mean()
+        assert abs(frac - p) < 6.0 * math.sqrt(p * (1 - p) / ((len(times) - 1) * 2 * M))
+    one = hs.reference_flip_bits_multi(3.0, [0.4], times, M, 2)
+    np.testing.assert_array_equal(one, hs.reference_flip_bits(3.0, 0.4, times, M, 2))
