@@ -133,6 +133,14 @@ int msgpu_upload_hamiltonian_csr(msgpu_ctx *ctx, int dim, const int *rowptr, con
 int msgpu_upload_hamiltonian_terms(msgpu_ctx *ctx, int dim, const int *rowptr, const int *col, int nterms,
                                    const double *vals, const double *coef);
 int msgpu_set_hamiltonian_coefficients(msgpu_ctx *ctx, const double *coef);
+/* Time-dependent H (dynamic interactions, TaskHSGeneral.cpp:486-560 with
+ * HSHamiltonianBuilder::BuildAtTime): coef holds nsteps rows of nterms
+ * coefficients, row j for global step first_step + j, evaluated by the caller
+ * at that step's midpoint; each step of msgpu_run then propagates with
+ * sum_k coef_k H_k, combined on the device.  Streamed Krylov and Taylor
+ * propagators; the dense propagator and the resident form need a static H.
+ * nsteps = 0 clears the schedule. */
+int msgpu_set_hamiltonian_schedule(msgpu_ctx *ctx, const double *coef, long long first_step, long long nsteps);
 
 /* K = kappa * I (symmetric recombination: kappa = k/2,
  * HSReactionRelaxation::BuildReactionForOrientation, HSReactionRelaxation.cpp:134-164). */

@@ -52,6 +52,10 @@ struct msgpu_ctx {
     DevBuf hterms, qsrc;   // nterms x nnz complex128; CSR index of every quartet value slot (-1: zero)
     size_t q_nslots = 0;
     std::array<double, 16> hcoef{};  // current coefficients
+    // time-dependent H: coefficients per global step (sched_steps x nterms),
+    // evaluated by the caller at each step's midpoint
+    std::vector<double> sched;
+    long long sched_first = 0, sched_steps = 0;
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
     int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
     // resident (one warp per trajectory, whole time loop per launch) form
@@ -769,7 +773,7 @@ constexpr int kResidentMaxDim = 1024;
 
 int resident_warps(const msgpu_ctx *c, int prec, int m)
 {
-    if (c->form == MSGPU_FORM_STREAMED) return 0;
+    if (c->form == MSGPU_FORM_STREAMED || c->sched_steps) return 0;  // a schedule changes H between launches
     if (prec == MSGPU_PREC_C64 && !c->k_scalar) return 0;
     if (c->form == MSGPU_FORM_AUTO && c->D > kResidentMaxDim) return 0;
     const size_t wb = resident_warp_bytes(c->D, m, prec == MSGPU_PREC_C128 ? 16 : 8);
@@ -1179,6 +1183,25 @@ int msgpu_set_hamiltonian_coefficients(msgpu_ctx *c, const double *coef)
     return MSGPU_OK;
 }
 
+int msgpu_set_hamiltonian_schedule(msgpu_ctx *c, const double *coef, long long first_step, long long nsteps)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    if (nsteps == 0) {
+        c->sched.clear();
+        c->sched_steps = 0;
+        return MSGPU_OK;
+    }
+    if (!c->terms) return fail(c, MSGPU_ERR_STATE, "Hamiltonian schedule: no terms uploaded");
+    if (!coef || nsteps < 0 || first_step < 0) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian schedule: invalid arguments");
+    const size_t n = static_cast<size_t>(nsteps) * c->nterms;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(coef[i])) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian schedule: non-finite coefficient");
+    c->sched.assign(coef, coef + n);
+    c->sched_first = first_step;
+    c->sched_steps = nsteps;
+    return MSGPU_OK;
+}
+
 int msgpu_upload_factors(msgpu_ctx *c, int dim, int ntraj, const double *factors)
 {
     return upload_factors_impl(c, dim, ntraj, factors, cudaMemcpyHostToDevice);
@@ -1225,7 +1248,11 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     for (int s = 0; s < p->ntimes; ++s)
         if (!std::isfinite(p->times[s]) || (s > 0 && !(p->times[s] > p->times[s - 1])))
             return fail(c, MSGPU_ERR_INVALID, "run: times must be finite and strictly increasing");
+    if (c->sched_steps && (p->step_offset < c->sched_first ||
+                           p->step_offset + (p->ntimes - 1) > c->sched_first + c->sched_steps))
+        return fail(c, MSGPU_ERR_INVALID, "run: the Hamiltonian schedule does not cover the requested steps");
     if (p->propagator == MSGPU_PROP_DENSE) {
+        if (c->sched_steps) return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator needs a time-independent H");
         if (p->precision != MSGPU_PREC_BF16X3 && p->precision != MSGPU_PREC_BF16X6)
             return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator takes MSGPU_PREC_BF16X3 or MSGPU_PREC_BF16X6");
         if (c->D > 4096) return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator is limited to dimension 4096");
@@ -1355,24 +1382,62 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     // Taylor propagator: the shift mu = trace(G)/D and a bound on ||G - mu I||_1
     double2 tmu = make_double2(0.0, 0.0);
     double tnorm = 0.0;
-    if (taylor) {
+    std::vector<double> term_stats;  // per term {tr.re, tr.im, max row sum} when a schedule drives H
+    if (taylor && c->sched_steps) {
+        if (int rc = ensure(c, c->work_d, 4 * sizeof(double), "Taylor statistics")) return rc;
+        term_stats.resize(3 * static_cast<size_t>(c->nterms));
+        for (int k = 0; k < c->nterms; ++k) {
+            CsrD Tk{Hd.rowptr, Hd.col, static_cast<const double2 *>(c->hterms.p) + static_cast<size_t>(k) * c->nnz};
+            k_g_stats<<<1, 256, 0, st>>>(Tk, D, static_cast<double *>(c->work_d.p));
+            if ((e = cudaMemcpyAsync(&term_stats[3 * k], c->work_d.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+                (e = cudaStreamSynchronize(st)))
+                return cuda_fail(c, e, "Taylor statistics");
+        }
+    }
+    // shift and norm bound of G - mu I from the H statistics {tr.re, tr.im, max row sum}
+    auto taylor_shift = [&](const double *hs) {
+        const double2 ktr = c->k_scalar ? make_double2(c->kappa * D, 0.0) : c->k_trace;
+        const double kn = c->k_scalar ? std::abs(c->kappa) : c->k_norm1;
+        // trace(G) = -i trace(H) - trace(K)
+        tmu = make_double2((hs[1] - ktr.x) / D, (-hs[0] - ktr.y) / D);
+        tnorm = hs[2] + kn + std::hypot(tmu.x, tmu.y);
+    };
+    if (taylor && !c->sched_steps) {
         if (int rc = ensure(c, c->work_d, 4 * sizeof(double), "Taylor statistics")) return rc;
         k_g_stats<<<1, 256, 0, st>>>(Hd, D, static_cast<double *>(c->work_d.p));
         double hs[3] = {0.0, 0.0, 0.0};
         if ((e = cudaMemcpyAsync(hs, c->work_d.p, sizeof(hs), cudaMemcpyDeviceToHost, st)) ||
             (e = cudaStreamSynchronize(st)))
             return cuda_fail(c, e, "Taylor statistics");
-        const double2 ktr = c->k_scalar ? make_double2(c->kappa * D, 0.0) : c->k_trace;
-        const double kn = c->k_scalar ? std::abs(c->kappa) : c->k_norm1;
-        // trace(G) = -i trace(H) - trace(K)
-        tmu = make_double2((hs[1] - ktr.x) / D, (-hs[0] - ktr.y) / D);
-        tnorm = hs[2] + kn + std::hypot(tmu.x, tmu.y);
+        taylor_shift(hs);
         if (!std::isfinite(tnorm)) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite Hamiltonian norm");
     }
     for (int s = 0; s < steps; ++s) {
         c->prof_tick = s;
         const double dt = p->times[s + 1] - p->times[s];
         const long long g = g0 + s;
+        if (c->sched_steps) {
+            // H at this step's midpoint from the schedule: combine the terms
+            // on the device, refresh the quartet values of the complex64 form
+            const double *row = c->sched.data() + static_cast<size_t>(g - c->sched_first) * c->nterms;
+            TermCoef cf;
+            std::memset(&cf, 0, sizeof(cf));
+            double hs[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < c->nterms; ++k) {
+                cf.c[k] = row[k];
+                if (taylor) {
+                    hs[0] += row[k] * term_stats[3 * k];
+                    hs[1] += row[k] * term_stats[3 * k + 1];
+                    hs[2] += std::abs(row[k]) * term_stats[3 * k + 2];  // norm bound of the combination
+                }
+            }
+            k_combine_terms<<<ceil_div(std::max(1, c->nnz), 256), 256, 0, st>>>(
+                static_cast<const double2 *>(c->hterms.p), c->nterms, cf, c->nnz, static_cast<double2 *>(c->hval.p),
+                static_cast<float2 *>(c->hhi.p), static_cast<float2 *>(c->hlo.p), static_cast<int *>(c->status.p));
+            if (prec == MSGPU_PREC_C64)
+                if (int rc = refresh_quartet_values(c)) return rc;
+            if (taylor) taylor_shift(hs);
+        }
         if ((e = cudaMemsetAsync(c->mdim.p, 0, ldm * sizeof(int), st))) return cuda_fail(c, e, "mdim reset");
         if (taylor) {
             // exp(dt (G - mu I)) by s sub-steps of a degree-mt Taylor series

@@ -127,6 +127,16 @@ class HSPropagatorB200:
         c = np.ascontiguousarray(coef, dtype=np.float64)
         _check(self.ctx, L.lib.msgpu_set_hamiltonian_coefficients(self.ctx, L.dptr(c)))
 
+    def set_hamiltonian_schedule(self, coef, first_step: int = 0):
+        """coef: (nsteps, nterms) coefficients, row j for global step first_step + j
+        (H at that step's midpoint); None clears the schedule."""
+        if coef is None:
+            _check(self.ctx, L.lib.msgpu_set_hamiltonian_schedule(self.ctx, None, 0, 0))
+            return
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        _check(self.ctx, L.lib.msgpu_set_hamiltonian_schedule(self.ctx, L.dptr(c.reshape(-1)), int(first_step),
+                                                              int(c.shape[0])))
+
     def set_reaction(self, kappa: float | None = None, csr=None):
         if csr is None:
             _check(self.ctx, L.lib.msgpu_set_reaction_scalar(self.ctx, float(kappa)))
