@@ -104,34 +104,18 @@ class ClockSampler:
 
 
 def _dist():
-    import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    torch.cuda.set_device(local)
-    return world, rank, local
+    from molspin_b200 import ranks
+    return ranks.init()
 
 
 def _max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from molspin_b200 import ranks
+    return ranks.max_over_ranks(x, world)
 
 
 def _barrier(world: int):
-    import torch
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
+    from molspin_b200 import ranks
+    ranks.barrier(world)
 
 
 def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
@@ -187,6 +171,7 @@ def run_ours(args):
 
     from molspin_b200 import _lib as L
     from molspin_b200 import hsgeneral as hs
+    from molspin_b200 import ranks
     from molspin_b200 import systems as S
 
     world, rank, local = _dist()
@@ -195,7 +180,7 @@ def run_ours(args):
     sysm = w.system
     D = sysm.dim
     rowptr, col, val = sysm.hamiltonian_csr()
-    F = sysm.trace_samples(M, w.seed + rank)
+    F = sysm.trace_samples(M, ranks.block_seed(w.seed, rank))
     obs = [(op, rate) for _, op, rate in sysm.observables()]
     times = S.time_grid(chunk * w.dt, w.dt)
     stream = torch.cuda.current_stream()
@@ -234,8 +219,7 @@ def run_ours(args):
     p.profile(False)
     launches = p.launch_count() - launches0
     el_max = _max_over_ranks(el_ms, world)
-    traj_steps = world * M * chunk * K
-    value = traj_steps / (el_max / 1e3)
+    value = ranks.aggregate(M * chunk * K, world, el_max / 1e3)
 
     # roofline of the dominant kernel (Lanczos SpMM): algorithmic bytes per
     # launch = read the block's Krylov vector once + write H v once (D*M*8 each)
@@ -333,9 +317,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    ranks.finish(world)
 
 
 def _peaks() -> dict:
@@ -634,6 +616,8 @@ def main():
         run_serving(args)
     else:
         run_ours(args)
+    from molspin_b200 import ranks
+    ranks.finish(int(os.environ.get("WORLD_SIZE", "1")))
 
 
 if __name__ == "__main__":
