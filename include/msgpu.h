@@ -67,6 +67,10 @@ extern "C" {
  * from a random norm estimate; this choice is deterministic and no less
  * accurate. */
 #define MSGPU_PROP_TAYLOR 2
+/* propagationmethod=rk4 (HSPropagator.cpp:80-90): one classical RK4 step of
+ * dB/dt = (-iH - K) B per time step, complex128, time-independent H; the
+ * explicit method needs dt small against 1/||H||. */
+#define MSGPU_PROP_RK4 3
 #define MSGPU_PREC_BF16X3 2
 #define MSGPU_PREC_BF16X6 3
 

@@ -31,6 +31,7 @@ REC_LANCZOS = 2
 PROP_KRYLOV = 0
 PROP_DENSE = 1
 PROP_TAYLOR = 2
+PROP_RK4 = 3
 OPT_TAYLOR_TOL = 2
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3

@@ -1265,14 +1265,17 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     }
     if (p->precision != MSGPU_PREC_C128 && p->precision != MSGPU_PREC_C64)
         return fail(c, MSGPU_ERR_INVALID, "run: unknown precision");
+    const bool rk4 = p->propagator == MSGPU_PROP_RK4;
     const bool taylor = p->propagator == MSGPU_PROP_TAYLOR;
-    if (p->propagator != MSGPU_PROP_KRYLOV && !taylor) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
-    if (taylor && p->precision != MSGPU_PREC_C128)
-        return fail(c, MSGPU_ERR_INVALID, "run: the Taylor propagator is complex128 only");
-    if (!taylor && (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov))
+    if (p->propagator != MSGPU_PROP_KRYLOV && !taylor && !rk4) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
+    if ((taylor || rk4) && p->precision != MSGPU_PREC_C128)
+        return fail(c, MSGPU_ERR_INVALID, "run: the Taylor and RK4 propagators are complex128 only");
+    if (rk4 && c->sched_steps)
+        return fail(c, MSGPU_ERR_INVALID, "run: the RK4 propagator takes a time-independent H (dynamic RK4 is not built)");
+    if (!taylor && !rk4 && (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov))
         return fail(c, MSGPU_ERR_INVALID, "run: krylov_dim must be in 1..32");
     int rec = p->recurrence;
-    if (rec == MSGPU_REC_AUTO || taylor)
+    if (rec == MSGPU_REC_AUTO || taylor || rk4)
         rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
     if (rec == MSGPU_REC_LANCZOS && !c->k_scalar)
         return fail(c, MSGPU_ERR_INVALID, "run: Lanczos requires a scalar reaction operator K");
@@ -1289,9 +1292,9 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     if (int rc = device_guard(c)) return rc;
 
     const int D = c->D, ldm = c->ldm, M = c->M;
-    const int m = taylor ? 1 : std::min(p->krylov_dim, D);  // the Taylor step needs no Krylov basis
+    const int m = (taylor || rk4) ? 1 : std::min(p->krylov_dim, D);  // no Krylov basis (RK4 uses slot 0 as its sum)
     const int prec = p->precision;
-    if (!taylor && resident_warps(c, prec, m) > 0) return run_resident(c, p, prec, m);
+    if (!taylor && !rk4 && resident_warps(c, prec, m) > 0) return run_resident(c, p, prec, m);
     if (c->form == MSGPU_FORM_RESIDENT)
         return fail(c, MSGPU_ERR_INVALID, "run: the resident form does not fit this dimension / recurrence / propagator");
     const int nobs = static_cast<int>(c->obs.size());
@@ -1468,6 +1471,26 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 Timed tm(c, KC_COMBINE);
                 k_combine<double2, false><<<qgrid, qblock, 0, st>>>(
                     F, nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz, g, 1, pstep(s),
+                    s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, static_cast<double *>(c->qpart_obs.p),
+                    static_cast<double *>(c->qpart_nrm.p));
+            }
+        } else if (rk4) {
+            double2 *psi = static_cast<double2 *>(c->psi128.p);
+            double2 *ya = static_cast<double2 *>(c->wbuf.p), *yb = static_cast<double2 *>(c->zbuf.p);
+            double2 *acc = static_cast<double2 *>(c->basis.p);
+            dim3 tgrid(ceil_div(D, 8), ldm / 32), tblock(32, 8);
+            const double cs[4] = {0.5 * dt, 0.5 * dt, dt, 0.0}, ws[4] = {dt / 6.0, dt / 3.0, dt / 3.0, dt / 6.0};
+            const double2 *in[4] = {psi, ya, yb, ya};
+            double2 *out[4] = {ya, yb, ya, nullptr};
+            for (int stage = 0; stage < 4; ++stage) {
+                Timed tm(c, KC_APPLY);
+                k_rk4_stage<<<tgrid, tblock, 0, st>>>(Hd, Kd, kappa, in[stage], psi, out[stage], acc, cs[stage],
+                                                      ws[stage], stage + 1, D, ldm);
+            }
+            {
+                Timed tm(c, KC_COMBINE);
+                k_combine<double2, false><<<qgrid, qblock, 0, st>>>(
+                    psi, nullptr, 0, nullptr, nullptr, mws, c->s1, c->s2, Q, ldm, QR, nz, g, 1, pstep(s),
                     s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, static_cast<double *>(c->qpart_obs.p),
                     static_cast<double *>(c->qpart_nrm.p));
             }

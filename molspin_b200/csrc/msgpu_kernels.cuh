@@ -534,6 +534,42 @@ k_taylor_term(CsrD H, CsrD K, double kappa, double2 mu, const double2 *__restric
     F[e] = make_double2(f.x + o.x, f.y + o.y);
 }
 
+// One stage of the classical RK4 step for dB/dt = G B (propagationmethod=rk4,
+// HSPropagator::Step, HSPropagator.cpp:80-90): k = G y_in at (row, trajectory),
+// then stage 1: acc = psi + w k, y_out = psi + c k; stages 2, 3: acc += w k,
+// y_out = psi + c k; stage 4: psi = acc + w k.  No stage writes a buffer it
+// gathers from (stage 1 reads psi, stage 4 writes it and reads y_in).
+__global__ void __launch_bounds__(256)
+k_rk4_stage(CsrD H, CsrD K, double kappa, const double2 *__restrict__ y_in, double2 *psi, double2 *__restrict__ y_out,
+            double2 *__restrict__ acc, double c, double w, int stage, int D, int ldm)
+{
+    const int t = blockIdx.y * 32 + threadIdx.x;
+    const int r = blockIdx.x * 8 + threadIdx.y;
+    if (r >= D) return;
+    double2 h = make_double2(0.0, 0.0);
+    for (int k = __ldg(H.rowptr + r); k < __ldg(H.rowptr + r + 1); ++k)
+        h = cfma(H.val[k], y_in[static_cast<size_t>(__ldg(H.col + k)) * ldm + t], h);
+    const size_t e = static_cast<size_t>(r) * ldm + t;
+    double2 g = make_double2(h.y, -h.x);  // -i (H y)_r
+    if (K.rowptr) {
+        double2 kk = make_double2(0.0, 0.0);
+        for (int k = __ldg(K.rowptr + r); k < __ldg(K.rowptr + r + 1); ++k)
+            kk = cfma(K.val[k], y_in[static_cast<size_t>(__ldg(K.col + k)) * ldm + t], kk);
+        g = csub(g, kk);
+    } else {
+        g = csub(g, cscale(y_in[e], kappa));
+    }
+    if (stage == 4) {
+        const double2 a = acc[e];
+        psi[e] = make_double2(a.x + w * g.x, a.y + w * g.y);
+        return;
+    }
+    const double2 p = psi[e];
+    y_out[e] = make_double2(p.x + c * g.x, p.y + c * g.y);
+    const double2 a = stage == 1 ? p : acc[e];
+    acc[e] = make_double2(a.x + w * g.x, a.y + w * g.y);
+}
+
 // End of a Taylor sub-step: F <- eta F (the shift e^{tau mu / s}), B <- F.
 __global__ void k_taylor_rescale(double2 *__restrict__ F, double2 *__restrict__ B, double2 eta, size_t n)
 {

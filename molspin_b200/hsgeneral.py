@@ -182,9 +182,9 @@ class HSPropagatorB200:
     def propagate(self, times: np.ndarray, krylov: int, precision: str = "c128", step_offset: int = 0,
                   accumulate: bool = False, recurrence: int = L.REC_AUTO, propagator: str = "krylov"):
         """propagator "krylov" (precision c128 | c64), "dense" (bf16x3 | bf16x6,
-        tensor cores) or "taylor" (c128; the reference's autoexpm)."""
+        tensor cores), "taylor" (c128; the reference's autoexpm) or "rk4" (c128, explicit)."""
         t = np.ascontiguousarray(times, dtype=np.float64)
-        prop = {"krylov": L.PROP_KRYLOV, "dense": L.PROP_DENSE, "taylor": L.PROP_TAYLOR}[propagator]
+        prop = {"krylov": L.PROP_KRYLOV, "dense": L.PROP_DENSE, "taylor": L.PROP_TAYLOR, "rk4": L.PROP_RK4}[propagator]
         p = L.RunParams(L.dptr(t), len(t), int(krylov), self.PRECISIONS[precision], int(recurrence), prop,
                         int(step_offset), 1 if accumulate else 0)
         _check(self.ctx, L.lib.msgpu_run(self.ctx, C.byref(p)))

@@ -587,7 +587,8 @@ int oracle_apply_st(int D, const int *urow, const int *ucol, const double *uval,
 // Full stochastic finite-time loop for one orientation.
 //   H: CSR (rad/ns); K: CSR or NULL with K = kappa I; G = -iH - K.
 //   factors: D x M column-major (re,im), overwritten with the final state.
-//   method: 0 = krylov (krylovsize kry), 1 = dense exponential of dt*G.
+//   method: 0 = krylov (krylovsize kry), 1 = dense exponential of dt*G,
+//     2 = classical RK4 on dB/dt = G B.
 //   noise: U CSR (NULL for none) with event rate lambda (= k_ST/2);
 //     noise_mode 0 = reference stream (seed, seed_mode, orientation as in
 //     oracle_st_flip_bits), 1 = explicit flip bits (same layout).
@@ -712,6 +713,20 @@ int oracle_hs_stochastic(int D, int M,
                 cd *x = &B[static_cast<size_t>(c) * D];
                 krylov_expm_general(G, x, dt, kry, y.data());
                 std::copy(y.begin(), y.end(), x);
+            });
+        } else if (method == 2) {
+            // classical RK4 for dB/dt = G B (HSPropagator.cpp:80-90)
+            parallel_cols([&](int c) {
+                cd *x = &B[static_cast<size_t>(c) * D];
+                std::vector<cd> k1(D), k2(D), k3(D), k4(D), y(D);
+                csr_matvec(G, x, k1.data());
+                for (int i = 0; i < D; ++i) y[i] = x[i] + 0.5 * dt * k1[i];
+                csr_matvec(G, y.data(), k2.data());
+                for (int i = 0; i < D; ++i) y[i] = x[i] + 0.5 * dt * k2[i];
+                csr_matvec(G, y.data(), k3.data());
+                for (int i = 0; i < D; ++i) y[i] = x[i] + dt * k3[i];
+                csr_matvec(G, y.data(), k4.data());
+                for (int i = 0; i < D; ++i) x[i] += (dt / 6.0) * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
             });
         } else {
             if (UpropDt != dt) {

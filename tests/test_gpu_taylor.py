@@ -77,3 +77,30 @@ def test_taylor_is_complex128_only():
         with pytest.raises(hs.MsgpuError) as e:
             p.propagate(S.time_grid(3.0, 1.0), 16, "c64", propagator="taylor")
         assert e.value.code == L.MSGPU_ERR_INVALID
+
+
+@pytest.mark.parametrize("form", ["streamed"])
+def test_rk4_against_oracle_restatement(form):
+    # the explicit RK4 step (propagationmethod=rk4) against the oracle's RK4,
+    # and its fourth-order convergence to the FP64 expm result
+    w = S.plain_small()
+    M = 32
+    F = w.system.trace_samples(M, w.seed)
+    errs = []
+    for dt in (0.2, 0.1):
+        times = S.time_grid(20.0, dt)
+        with hs.HSPropagatorB200(0) as p:
+            p.set_form(form)
+            p.set_hamiltonian(*w.system.hamiltonian_csr())
+            p.set_reaction(kappa=w.system.kappa())
+            p.set_electron_pair(*w.system.electron_strides())
+            p.set_observables([(op, rate) for _, op, rate in w.system.observables()])
+            p.set_factors(F)
+            p.propagate(times, 16, "c128", propagator="rk4")
+            per, _ = p.yields()
+        obs = h.oracle_observables(w.system)
+        rk = orc.hs_stochastic(w.system.hamiltonian_csr(), F, times, obs, kappa=w.system.kappa(), method=2, nthreads=8)
+        ex = orc.hs_stochastic(w.system.hamiltonian_csr(), F, times, obs, kappa=w.system.kappa(), method=1, nthreads=8)
+        assert _rel(per, rk["traj_yield"]) < 1e-11
+        errs.append(_rel(per, ex["traj_yield"]))
+    assert errs[1] < errs[0] / 10  # fourth order: about 16x per halving
