@@ -78,6 +78,10 @@ extern "C" {
 #define MSGPU_OPT_DENSE_RENORMALIZE 1 /* 1 (default): the dense form restores the exact
                                         Haberkorn survival |psi|^2 e^{-2 kappa t} of each
                                         trajectory every step (scalar K only); 0: off */
+#define MSGPU_OPT_SPMM_VARIANT 3      /* -1 (default): the autotuner picks the complex64 SpMM
+                                        variant and tile; k >= 0: tune the tile of variant k
+                                        only (0-3 register-gather variants, 4-5 the variants
+                                        that stage the tile's own quartets in shared memory) */
 #define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
                                         (default, "double"), 2^-24 ("single"), 2^-10 ("half") */
 

@@ -33,6 +33,7 @@ PROP_DENSE = 1
 PROP_TAYLOR = 2
 PROP_RK4 = 3
 OPT_TAYLOR_TOL = 2
+OPT_SPMM_VARIANT = 3
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
 OPT_DENSE_RENORMALIZE = 1

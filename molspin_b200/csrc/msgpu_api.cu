@@ -21,6 +21,7 @@ using namespace msgpu;
 namespace {
 
 enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_N = 7 };
+constexpr int kNumSpmmVariants = 6;  // entries of kApplyVariants (checked there)
 
 struct DevBuf {
     void *p = nullptr;
@@ -71,6 +72,7 @@ struct msgpu_ctx {
     double2 k_trace = {0.0, 0.0};  // trace of a CSR K
     double k_norm1 = 0.0;          // its 1-norm (max column sum)
     double taylor_tol = 0x1p-53;   // MSGPU_OPT_TAYLOR_TOL
+    int spmm_variant = -1;         // MSGPU_OPT_SPMM_VARIANT (-1: autotuned)
     DevBuf krow, kcol, kval;
     // electron pair
     int s1 = 0, s2 = 0;
@@ -282,6 +284,13 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
     if (!c) return MSGPU_ERR_INVALID;
     if (key == MSGPU_OPT_DENSE_RENORMALIZE) {
         c->dense_renorm = value != 0.0;
+        return MSGPU_OK;
+    }
+    if (key == MSGPU_OPT_SPMM_VARIANT) {
+        const int v = static_cast<int>(value);
+        if (v < -1 || v >= kNumSpmmVariants || v != value) return fail(c, MSGPU_ERR_INVALID, "SpMM variant out of range");
+        c->spmm_variant = v;
+        c->q_tile = 0;  // tune again among the allowed variants
         return MSGPU_OK;
     }
     if (key == MSGPU_OPT_TAYLOR_TOL) {
@@ -1062,13 +1071,42 @@ QuartetC quartet_view(const msgpu_ctx *c)
 // CTA) on the context's own data with CUDA events and keeps the fastest for
 // this (D, trajectory block).  Runs once per context and shape.
 using ApplyFn = void (*)(QuartetC, const float2 *, const double *, float2 *, double *, int, int, int, int, int);
-const ApplyFn kApplyVariants[] = {
-    k_lanczos_apply_compact<true, 2>,
-    k_lanczos_apply_compact<true, 3>,
-    k_lanczos_apply_compact<false, 3>,
-    k_lanczos_apply_compact<false, 4>,
+struct ApplyVariant {
+    ApplyFn fn;
+    bool cube;  // stages the tile's own input quartets in shared memory (QT x 2 KB)
+};
+const ApplyVariant kApplyVariants[] = {
+    {k_lanczos_apply_compact<true, 2>, false},
+    {k_lanczos_apply_compact<true, 3>, false},
+    {k_lanczos_apply_compact<false, 3>, false},
+    {k_lanczos_apply_compact<false, 4>, false},
+    {k_lanczos_apply_cube<2>, true},
+    {k_lanczos_apply_cube<3>, true},
 };
 constexpr int kNumApplyVariants = sizeof(kApplyVariants) / sizeof(kApplyVariants[0]);
+static_assert(kNumApplyVariants == kNumSpmmVariants, "SpMM variant count");
+constexpr int kCubeMaxQT = 64;  // 128 KB of shared memory
+
+// Whether variant v can run with tile QT on this system, and its shared memory.
+bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
+{
+    *smem = 0;
+    if (!kApplyVariants[v].cube) return true;
+    // the tile's quartet bases must be contiguous: QT divides the second stride
+    if (qt > kCubeMaxQT || c->s2 % qt != 0) return false;
+    *smem = static_cast<size_t>(qt) * 4 * 32 * sizeof(float4);
+    return true;
+}
+
+void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st, const float2 *w, const double *s,
+                  float2 *U, double *part)
+{
+    size_t smem = 0;
+    apply_fits(c, v, qt, &smem);
+    if (smem) cudaFuncSetAttribute(kApplyVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    kApplyVariants[v].fn<<<grid, kThreads, smem, st>>>(quartet_view(c), w, s, U, part, c->D / 4, c->s1, c->s2, c->ldm,
+                                                       qt);
+}
 
 int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U, double *part)
 {
@@ -1082,20 +1120,21 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
     // its best round: a one-off delay (another stream, a profiler) then cannot
     // pick the shape
     std::vector<std::pair<int, int>> cands;
-    for (int v = 0; v < kNumApplyVariants; ++v)
+    size_t smem;
+    for (int v = 0; v < kNumApplyVariants; ++v) {
+        if (c->spmm_variant >= 0 && v != c->spmm_variant) continue;
         for (int qt : cand)
-            if (qt <= Q || qt == cand[0]) cands.push_back({v, qt});
+            if ((qt <= Q || qt == cand[0]) && apply_fits(c, v, qt, &smem)) cands.push_back({v, qt});
+    }
+    if (cands.empty()) return fail(c, MSGPU_ERR_INVALID, "SpMM variant does not fit this system");
     std::vector<float> score(cands.size(), 1e30f);
     for (int round = 0; round < 3; ++round)
         for (size_t k = 0; k < cands.size(); ++k) {
             const int v = cands[k].first, qt = cands[k].second;
             dim3 grid(ceil_div(Q, qt), c->ldm / 64);
-            kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
-                                                                c->ldm, qt);
+            launch_apply(c, v, qt, grid, c->stream, w, s, U, part);
             cudaEventRecord(a, c->stream);
-            for (int rep = 0; rep < 2; ++rep)
-                kApplyVariants[v]<<<grid, kThreads, 0, c->stream>>>(quartet_view(c), w, s, U, part, Q, c->s1, c->s2,
-                                                                    c->ldm, qt);
+            for (int rep = 0; rep < 2; ++rep) launch_apply(c, v, qt, grid, c->stream, w, s, U, part);
             cudaEventRecord(b, c->stream);
             cudaEventSynchronize(b);
             float ms = 0.f;
@@ -1563,8 +1602,8 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             for (int j = 0; j < m; ++j) {
                 {
                     Timed tm(c, KC_APPLY);
-                    kApplyVariants[c->q_variant]<<<qgrid_apply, kThreads, 0, st>>>(
-                        quartet_view(c), Wb + j * n, sc + static_cast<size_t>(j) * ldm, U, part, Q, c->s1, c->s2, ldm, QT);
+                    launch_apply(c, c->q_variant, QT, qgrid_apply, st, Wb + j * n, sc + static_cast<size_t>(j) * ldm, U,
+                                 part);
                 }
                 {
                     Timed tm(c, KC_REDUCE);

@@ -372,6 +372,80 @@ k_lanczos_apply_compact(QuartetC H, const float2 *__restrict__ wj, const double 
     }
 }
 
+// Variant of k_lanczos_apply_compact that first stages the CTA's own input
+// quartets (its QT output quartets x 64 trajectories, 4 rows each, 16 bytes
+// a lane) in shared memory with cp.async: the diagonal block and every
+// nucleus flip that stays inside the tile (the low quartet-index bits) then
+// read shared memory instead of gathering from L2; the rest gathers as
+// before.  Needs the tile's quartet bases to be contiguous (QT divides s2),
+// which the host checks; dynamic shared memory QT x 4 x 512 bytes.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_lanczos_apply_cube(QuartetC H, const float2 *__restrict__ wj, const double *__restrict__ sj, float2 *__restrict__ U,
+                     double *__restrict__ part, int Q, int s1, int s2, int ldm, int QT)
+{
+    extern __shared__ float4 cube[];  // [QT * 4 rows][32 lanes]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 64 + 2 * lane;
+    const int q0 = blockIdx.x * QT;
+    const int nq = min(QT, Q - q0);
+    const int base0 = __ldg(H.base + q0);
+    const int off[4] = {0, s2, s1, s1 + s2};
+    // stage: row slot i = 4 j + a holds quartet q0 + j, offset a
+    for (int i = warp; i < 4 * nq; i += kWarps) {
+        const int j = i >> 2, a = i & 3;
+        const float4 *src = reinterpret_cast<const float4 *>(wj + static_cast<size_t>(base0 + j + off[a]) * ldm + t);
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(cube + i * 32 + lane));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const float sc0 = static_cast<float>(sj[t]), sc1 = static_cast<float>(sj[t + 1]);
+    double a0 = 0.0, a1 = 0.0;
+    for (int q = q0 + warp; q < q0 + nq; q += kWarps) {
+        float2 o[4][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) o[a][0] = o[a][1] = make_float2(0.f, 0.f);
+        const int kb = __ldg(H.rowptr + q), ke = __ldg(H.rowptr + q + 1);
+        for (int k = kb; k < ke; ++k) {
+            const int2 cur = __ldg(H.blk + k);
+            const int cb = cur.x >> 3;
+            const unsigned rel = static_cast<unsigned>(cb - base0);
+            float4 x[4];
+            if (rel < static_cast<unsigned>(nq)) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b) x[b] = cube[(4 * rel + b) * 32 + lane];
+            } else {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    x[b] = *reinterpret_cast<const float4 *>(wj + static_cast<size_t>(cb + off[b]) * ldm + t);
+            }
+            quartet_block(o, cur.x & 7, H.val + cur.y, x);
+        }
+        const int jq = q - q0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const size_t e = static_cast<size_t>(base0 + jq + off[a]) * ldm + t;
+            const float2 ure = make_float2(o[a][0].x * sc0, o[a][0].y * sc1);
+            const float2 uim = make_float2(o[a][1].x * sc0, o[a][1].y * sc1);
+            *reinterpret_cast<float4 *>(U + e) = make_float4(ure.x, ure.y, uim.x, uim.y);
+            const float4 v = cube[(4 * jq + a) * 32 + lane];  // {re t, re t+1, im t, im t+1}
+            a0 += (static_cast<double>(v.x) * ure.x + static_cast<double>(v.z) * uim.x) * sc0;
+            a1 += (static_cast<double>(v.y) * ure.y + static_cast<double>(v.w) * uim.y) * sc1;
+        }
+    }
+    __shared__ double sm[kWarps][64];
+    sm[warp][2 * lane] = a0;
+    sm[warp][2 * lane + 1] = a1;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; ++w) s += sm[w][threadIdx.x];
+        part[static_cast<size_t>(blockIdx.x) * ldm + blockIdx.y * 64 + threadIdx.x] = s;
+    }
+}
+
 // w_{j+1} = U - alpha_j v_j - beta_j v_{j-1}; partial |w_{j+1}|^2 (FP64).
 __global__ void __launch_bounds__(kThreads)
 k_lanczos_update(const float2 *__restrict__ U, const float2 *__restrict__ wj, const float2 *__restrict__ wjm1,

@@ -245,3 +245,34 @@ def test_multi_term_dephasing_stream_replayed():
     per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
     ref = _oracle(system, F, times, 16, U=True, kappa=system.kappa(), noise_mode=1, flip_bits=bits)
     assert _rel(per, ref["traj_yield"]) < 1e-10
+
+
+@pytest.mark.parametrize("variant", [4, 5])
+def test_shared_memory_spmm_variants(variant):
+    # the SpMM variants that stage the tile's own quartets in shared memory,
+    # forced: complex64 against complex128 within the precision form's 1e-6
+    # and against the register-gather variant to FP32 rounding
+    system = h.random_system([2] * 5, [2] * 3, seed=71, aniso=True, st_rate=0.05)  # D = 1024
+    M, times = 128, S.time_grid(30.0, 1.0)
+    F = system.trace_samples(M, 2.0)
+    noise = (system.st_rate, L.NOISE_PHILOX, 5)
+
+    def run(precision, v):
+        with hs.HSPropagatorB200(0) as p:
+            p.set_form("streamed")
+            if v is not None:
+                p.set_option(L.OPT_SPMM_VARIANT, v)
+            p.set_hamiltonian(*system.hamiltonian_csr())
+            p.set_reaction(kappa=system.kappa())
+            p.set_electron_pair(*system.electron_strides())
+            p.set_observables([(op, rate) for _, op, rate in system.observables()])
+            p.set_noise(*noise)
+            p.set_factors(F)
+            p.propagate(times, 16, precision)
+            return p.yields()[0]
+
+    cube = run("c64", variant)
+    ref128 = run("c128", None)
+    reg = run("c64", 3)
+    assert _rel(cube, ref128) < 1e-6
+    assert _rel(cube, reg) < 1e-6
