@@ -81,7 +81,8 @@ extern "C" {
 #define MSGPU_OPT_SPMM_VARIANT 3      /* -1 (default): the autotuner picks the complex64 SpMM
                                         variant and tile; k >= 0: tune the tile of variant k
                                         only (0-3 register-gather variants, 4-5 the variants
-                                        that stage the tile's own quartets in shared memory) */
+                                        that stage the tile's own quartets in shared memory,
+                                        6-7 two trajectory pairs per thread) */
 #define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
                                         (default, "double"), 2^-24 ("single"), 2^-10 ("half") */
 

@@ -21,7 +21,7 @@ using namespace msgpu;
 namespace {
 
 enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_N = 7 };
-constexpr int kNumSpmmVariants = 6;  // entries of kApplyVariants (checked there)
+constexpr int kNumSpmmVariants = 8;  // entries of kApplyVariants (checked there)
 
 struct DevBuf {
     void *p = nullptr;
@@ -1074,14 +1074,17 @@ using ApplyFn = void (*)(QuartetC, const float2 *, const double *, float2 *, dou
 struct ApplyVariant {
     ApplyFn fn;
     bool cube;  // stages the tile's own input quartets in shared memory (QT x 2 KB)
+    int np;     // trajectory pairs per thread (a CTA covers 64 np trajectories)
 };
 const ApplyVariant kApplyVariants[] = {
-    {k_lanczos_apply_compact<true, 2>, false},
-    {k_lanczos_apply_compact<true, 3>, false},
-    {k_lanczos_apply_compact<false, 3>, false},
-    {k_lanczos_apply_compact<false, 4>, false},
-    {k_lanczos_apply_cube<2>, true},
-    {k_lanczos_apply_cube<3>, true},
+    {k_lanczos_apply_compact<true, 2>, false, 1},
+    {k_lanczos_apply_compact<true, 3>, false, 1},
+    {k_lanczos_apply_compact<false, 3>, false, 1},
+    {k_lanczos_apply_compact<false, 4>, false, 1},
+    {k_lanczos_apply_cube<2>, true, 1},
+    {k_lanczos_apply_cube<3>, true, 1},
+    {k_lanczos_apply_np<2, 2>, false, 2},
+    {k_lanczos_apply_np<2, 3>, false, 2},
 };
 constexpr int kNumApplyVariants = sizeof(kApplyVariants) / sizeof(kApplyVariants[0]);
 static_assert(kNumApplyVariants == kNumSpmmVariants, "SpMM variant count");
@@ -1091,6 +1094,7 @@ constexpr int kCubeMaxQT = 64;  // 128 KB of shared memory
 bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 {
     *smem = 0;
+    if (c->ldm % (64 * kApplyVariants[v].np) != 0) return false;
     if (!kApplyVariants[v].cube) return true;
     // the tile's quartet bases must be contiguous: QT divides the second stride
     if (qt > kCubeMaxQT || c->s2 % qt != 0) return false;
@@ -1103,6 +1107,7 @@ void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st,
 {
     size_t smem = 0;
     apply_fits(c, v, qt, &smem);
+    grid.y = c->ldm / (64 * kApplyVariants[v].np);
     if (smem) cudaFuncSetAttribute(kApplyVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     kApplyVariants[v].fn<<<grid, kThreads, smem, st>>>(quartet_view(c), w, s, U, part, c->D / 4, c->s1, c->s2, c->ldm,
                                                        qt);

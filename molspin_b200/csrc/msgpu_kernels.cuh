@@ -372,6 +372,161 @@ k_lanczos_apply_compact(QuartetC H, const float2 *__restrict__ wj, const double 
     }
 }
 
+// quartet_block for NP trajectory pairs per thread: the block's values are
+// loaded and broadcast once and applied to every pair.
+template <int NP>
+__device__ __forceinline__ void quartet_block_np(float2 (&o)[NP][4][2], int type, const float4 *__restrict__ v,
+                                                 const float4 (&x)[NP][4])
+{
+    switch (type) {
+    case 0:
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float4 p = __ldg(v + 2 * a), q = __ldg(v + 2 * a + 1);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                mac_pp(o[k][a], p.x, p.y, x[k][0]);
+                mac_pp(o[k][a], p.z, p.w, x[k][1]);
+                mac_pp(o[k][a], q.x, q.y, x[k][2]);
+                mac_pp(o[k][a], q.z, q.w, x[k][3]);
+            }
+        }
+        break;
+    case 1:
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2)
+#pragma unroll
+            for (int a1 = 0; a1 < 2; ++a1) {
+                const float4 p = __ldg(v + 2 * a2 + a1);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    mac_pp(o[k][2 * a1 + a2], p.x, p.y, x[k][a2]);
+                    mac_pp(o[k][2 * a1 + a2], p.z, p.w, x[k][2 + a2]);
+                }
+            }
+        break;
+    case 2:
+#pragma unroll
+        for (int a1 = 0; a1 < 2; ++a1)
+#pragma unroll
+            for (int a2 = 0; a2 < 2; ++a2) {
+                const float4 p = __ldg(v + 2 * a1 + a2);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    mac_pp(o[k][2 * a1 + a2], p.x, p.y, x[k][2 * a1]);
+                    mac_pp(o[k][2 * a1 + a2], p.z, p.w, x[k][2 * a1 + 1]);
+                }
+            }
+        break;
+    case 3: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            mac_pp(o[k][0], p.x, p.y, x[k][0]);
+            mac_pp(o[k][1], p.z, p.w, x[k][1]);
+            mac_pp(o[k][2], q.x, q.y, x[k][2]);
+            mac_pp(o[k][3], q.z, q.w, x[k][3]);
+        }
+        break;
+    }
+    case 4: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);  // A00 A01 | A10 A11
+#pragma unroll
+        for (int k = 0; k < NP; ++k)
+#pragma unroll
+            for (int a2 = 0; a2 < 2; ++a2) {
+                mac_pp(o[k][a2], p.x, p.y, x[k][a2]);
+                mac_pp(o[k][a2], p.z, p.w, x[k][2 + a2]);
+                mac_pp(o[k][2 + a2], q.x, q.y, x[k][a2]);
+                mac_pp(o[k][2 + a2], q.z, q.w, x[k][2 + a2]);
+            }
+        break;
+    }
+    default: {
+        const float4 p = __ldg(v), q = __ldg(v + 1);
+#pragma unroll
+        for (int k = 0; k < NP; ++k)
+#pragma unroll
+            for (int a1 = 0; a1 < 2; ++a1) {
+                mac_pp(o[k][2 * a1], p.x, p.y, x[k][2 * a1]);
+                mac_pp(o[k][2 * a1], p.z, p.w, x[k][2 * a1 + 1]);
+                mac_pp(o[k][2 * a1 + 1], q.x, q.y, x[k][2 * a1]);
+                mac_pp(o[k][2 * a1 + 1], q.z, q.w, x[k][2 * a1 + 1]);
+            }
+        break;
+    }
+    }
+}
+
+// Variant of k_lanczos_apply_compact with NP trajectory pairs per thread:
+// lane l holds pairs (t0 + 2 l + 64 k, +1), k < NP, so a CTA covers 64 NP
+// trajectories (ldm must be a multiple of 64 NP) and the block descriptors,
+// values and addresses serve NP pairs.  Same arithmetic per trajectory.
+template <int NP, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_lanczos_apply_np(QuartetC H, const float2 *__restrict__ wj, const double *__restrict__ sj, float2 *__restrict__ U,
+                   double *__restrict__ part, int Q, int s1, int s2, int ldm, int QT)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tb = blockIdx.y * 64 * NP + 2 * lane;
+    const int q0 = blockIdx.x * QT;
+    float sc[NP][2];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        sc[k][0] = static_cast<float>(sj[tb + 64 * k]);
+        sc[k][1] = static_cast<float>(sj[tb + 64 * k + 1]);
+    }
+    const int off[4] = {0, s2, s1, s1 + s2};
+    double acc[NP][2];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc[k][0] = acc[k][1] = 0.0;
+    for (int q = q0 + warp; q < min(q0 + QT, Q); q += kWarps) {
+        float2 o[NP][4][2];
+#pragma unroll
+        for (int k = 0; k < NP; ++k)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) o[k][a][0] = o[k][a][1] = make_float2(0.f, 0.f);
+        const int kb = __ldg(H.rowptr + q), ke = __ldg(H.rowptr + q + 1);
+        for (int kk = kb; kk < ke; ++kk) {
+            const int2 cur = __ldg(H.blk + kk);
+            float4 x[NP][4];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const float2 *row = wj + static_cast<size_t>((cur.x >> 3) + off[b]) * ldm + tb;
+#pragma unroll
+                for (int k = 0; k < NP; ++k) x[k][b] = *reinterpret_cast<const float4 *>(row + 64 * k);
+            }
+            quartet_block_np<NP>(o, cur.x & 7, H.val + cur.y, x);
+        }
+        const int base = __ldg(H.base + q);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const size_t e = static_cast<size_t>(base + off[a]) * ldm + tb;
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const float2 ure = make_float2(o[k][a][0].x * sc[k][0], o[k][a][0].y * sc[k][1]);
+                const float2 uim = make_float2(o[k][a][1].x * sc[k][0], o[k][a][1].y * sc[k][1]);
+                *reinterpret_cast<float4 *>(U + e + 64 * k) = make_float4(ure.x, ure.y, uim.x, uim.y);
+                const float4 v = *reinterpret_cast<const float4 *>(wj + e + 64 * k);
+                acc[k][0] += (static_cast<double>(v.x) * ure.x + static_cast<double>(v.z) * uim.x) * sc[k][0];
+                acc[k][1] += (static_cast<double>(v.y) * ure.y + static_cast<double>(v.w) * uim.y) * sc[k][1];
+            }
+        }
+    }
+    __shared__ double sm[kWarps][64 * NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        sm[warp][64 * k + 2 * lane] = acc[k][0];
+        sm[warp][64 * k + 2 * lane + 1] = acc[k][1];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 64 * NP; i += kThreads) {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; ++w) s += sm[w][i];
+        part[static_cast<size_t>(blockIdx.x) * ldm + blockIdx.y * 64 * NP + i] = s;
+    }
+}
+
 // Variant of k_lanczos_apply_compact that first stages the CTA's own input
 // quartets (its QT output quartets x 64 trajectories, 4 rows each, 16 bytes
 // a lane) in shared memory with cp.async: the diagonal block and every

@@ -247,7 +247,7 @@ def test_multi_term_dephasing_stream_replayed():
     assert _rel(per, ref["traj_yield"]) < 1e-10
 
 
-@pytest.mark.parametrize("variant", [4, 5])
+@pytest.mark.parametrize("variant", [4, 5, 6, 7])
 def test_shared_memory_spmm_variants(variant):
     # the SpMM variants that stage the tile's own quartets in shared memory,
     # forced: complex64 against complex128 within the precision form's 1e-6
