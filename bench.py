@@ -48,6 +48,8 @@ def _args():
     ap.add_argument("--requests", type=int, default=40, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=4.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6")
+    ap.add_argument("--spmm-variant", type=int, default=-1,
+                    help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
     return ap.parse_args()
 
 
@@ -187,6 +189,8 @@ def run_ours(args):
 
     p = hs.HSPropagatorB200(local)
     L.lib.msgpu_set_stream(p.ctx, stream.cuda_stream)
+    if args.spmm_variant >= 0:
+        p.set_option(L.OPT_SPMM_VARIANT, args.spmm_variant)
     p.set_hamiltonian(rowptr, col, val)
     p.set_reaction(kappa=sysm.kappa())
     p.set_electron_pair(*sysm.electron_strides())
@@ -300,7 +304,7 @@ def run_ours(args):
                        "krylov": w.krylov, "dt_ns": w.dt, "time_steps_per_bench_step": chunk,
                        "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos",
                        "parallelism": f"independent trajectory blocks x{world}"},
-            "roofline": {"bound": "hbm", "kernel": "k_lanczos_apply_compact", "achieved": achieved, "peak": hbm_peak,
+            "roofline": {"bound": "hbm", "kernel": "quartet SpMM (k_lanczos_apply_*, autotuned variant)", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": traffic,
                          "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": apply_avg_s * 1e3, "launches_timed": apply_n,
