@@ -38,3 +38,12 @@ def test_null_context_errors():
     assert L.lib.msgpu_last_error(None) == b"null context"
     assert L.lib.msgpu_run(None, None) == L.MSGPU_ERR_INVALID
     assert L.lib.msgpu_upload_hamiltonian_csr(None, 4, None, None, None) == L.MSGPU_ERR_INVALID
+
+
+def test_package_import_does_not_load_the_library():
+    # a fresh checkout builds through `python -m molspin_b200.build`, which
+    # imports the package before libmsgpu.so exists
+    code = ("import sys, molspin_b200, molspin_b200.build; "
+            "assert 'molspin_b200._lib' not in sys.modules; "
+            "molspin_b200.HSPropagatorB200; assert 'molspin_b200._lib' in sys.modules")
+    subprocess.run([os.sys.executable, "-c", code], cwd=ROOT, check=True)
