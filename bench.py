@@ -50,6 +50,9 @@ def _args():
     ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6")
     ap.add_argument("--spmm-variant", type=int, default=-1,
                     help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
+    ap.add_argument("--lanczos-cluster", type=int, default=0,
+                    help="precision form: 0 four-kernel Lanczos iteration (default); -1, 1, 2, 4, 8, 16 the "
+                         "cluster-resident recurrence (MSGPU_OPT_LANCZOS_CLUSTER)")
     return ap.parse_args()
 
 
@@ -191,6 +194,8 @@ def run_ours(args):
     L.lib.msgpu_set_stream(p.ctx, stream.cuda_stream)
     if args.spmm_variant >= 0:
         p.set_option(L.OPT_SPMM_VARIANT, args.spmm_variant)
+    if args.lanczos_cluster:
+        p.set_option(L.OPT_LANCZOS_CLUSTER, args.lanczos_cluster)
     p.set_hamiltonian(rowptr, col, val)
     p.set_reaction(kappa=sysm.kappa())
     p.set_electron_pair(*sysm.electron_strides())
@@ -220,6 +225,7 @@ def run_ours(args):
     apply_ms, apply_n = p.profile_read(L.KC_APPLY)
     orth_ms, orth_n = p.profile_read(L.KC_ORTH)
     comb_ms, comb_n = p.profile_read(L.KC_COMBINE)
+    fused_ms, fused_n = p.profile_read(L.KC_LANCZOS)
     p.profile(False)
     launches = p.launch_count() - launches0
     el_max = _max_over_ranks(el_ms, world)
@@ -311,7 +317,9 @@ def run_ours(args):
                          "timing": "CUDA events around every launch of every 8th time step (sampled)",
                          "share_of_step": apply_avg_s * 1e3 * w.krylov * chunk * K / el_ms if el_ms else None},
             "kernel_avg_ms": {"apply": apply_ms / max(1, apply_n), "update": orth_ms / max(1, orth_n),
-                              "combine": comb_ms / max(1, comb_n)},
+                              "combine": comb_ms / max(1, comb_n),
+                              **({"lanczos_cluster_resident": fused_ms / fused_n} if fused_n else {})},
+            "lanczos": "cluster-resident recurrence" if fused_n else "SpMM + update + reductions per iteration",
             "plain_c128": {"value": plain_value, "unit": "traj-steps/s", "steps": plain_steps,
                            "speedup_of_c64": (value / world / plain_value) if plain_value else None},
             "yield_rel_err_c64_vs_c128": yerr,

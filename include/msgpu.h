@@ -82,9 +82,21 @@ extern "C" {
                                         variant and tile; k >= 0: tune the tile of variant k
                                         only (0-3 register-gather variants, 4-5 the variants
                                         that stage the tile's own quartets in shared memory,
-                                        6-7 two trajectory pairs per thread) */
+                                        6-7 two trajectory pairs per thread); a forced variant
+                                        also keeps the four-kernel Lanczos iteration */
 #define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
                                         (default, "double"), 2^-24 ("single"), 2^-10 ("half") */
+#define MSGPU_OPT_LANCZOS_CLUSTER 4   /* complex64 streamed form.  0 (default): per Krylov
+                                        iteration one SpMM, one update and two reductions.
+                                        -1: the whole Lanczos recurrence of a step as one
+                                        cluster-resident launch (two trajectory pairs per
+                                        thread-block cluster, their vectors in shared memory)
+                                        with the smallest cluster of at most 16 CTAs that
+                                        holds them (not while MSGPU_OPT_SPMM_VARIANT forces a
+                                        variant); 1, 2, 4, 8 or 16: that cluster size only.
+                                        Same results to FP32 rounding; at D=16384 with 1024
+                                        trajectories on a B200 it is the slower of the two
+                                        (latency-bound at one 512-thread CTA per SM) */
 
 /* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
  * dimensions (the whole time loop in one launch, one warp per trajectory,
@@ -196,7 +208,8 @@ int msgpu_fetch_values(msgpu_ctx *ctx, double *values);
 
 /* Kernel timing with CUDA events on the launch stream.  Classes:
  * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield,
- * 6 dense GEMM (tensor cores).  enable: 0 off; 1 every launch; 2 sampled --
+ * 6 dense GEMM (tensor cores), 7 cluster-resident Lanczos recurrence (one
+ * launch per step, MSGPU_OPT_LANCZOS_CLUSTER).  enable: 0 off; 1 every launch; 2 sampled --
  * every launch of every 8th time step of the streamed step loop, and every
  * 8th dense GEMM (events between kernels cost them their overlap, so timing
  * every launch slows a many-launch step by about 10 %; the sampled mode

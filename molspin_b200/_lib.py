@@ -34,6 +34,7 @@ PROP_TAYLOR = 2
 PROP_RK4 = 3
 OPT_TAYLOR_TOL = 2
 OPT_SPMM_VARIANT = 3
+OPT_LANCZOS_CLUSTER = 4
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
 OPT_DENSE_RENORMALIZE = 1
@@ -44,7 +45,7 @@ FORM_AUTO = 0
 FORM_STREAMED = 1
 FORM_RESIDENT = 2
 
-KC_APPLY, KC_ORTH, KC_REDUCE, KC_EXPM, KC_COMBINE, KC_YIELD = range(6)
+KC_APPLY, KC_ORTH, KC_REDUCE, KC_EXPM, KC_COMBINE, KC_YIELD, KC_GEMM, KC_LANCZOS = range(8)
 
 
 class RunParams(C.Structure):

@@ -8,11 +8,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "msgpu_dense.h"
+#include "msgpu_fused.cuh"
 #include "msgpu_kernels.cuh"
 #include "msgpu_resident.cuh"
 
@@ -20,7 +22,10 @@ using namespace msgpu;
 
 namespace {
 
-enum KClass { KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_N = 7 };
+enum KClass {
+    KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_LANCZOS = 7,
+    KC_N = 8
+};
 constexpr int kNumSpmmVariants = 8;  // entries of kApplyVariants (checked there)
 
 struct DevBuf {
@@ -46,6 +51,18 @@ struct msgpu_ctx {
     // quartet-block form of H for the current electron strides
     DevBuf qrow, qcolt, qval, qbase;
     int q_s1 = 0, q_s2 = 0, q_D = 0, q_nblocks = 0;
+    long long q_build = 0;            // counts quartet-form builds
+    std::vector<int> q_hrow;          // host copies of the quartet form
+    std::vector<int2> q_hblk;
+    std::vector<float> q_hval;
+    // cluster-resident complex64 Lanczos (k_lanczos_fused): descriptors for
+    // cluster size f_C, built from quartet build f_build
+    DevBuf fblk, fval, frow, fdsrc, fdiag;
+    int f_C = 0, f_nblk_max = 0, f_opt = 0;  // f_opt: MSGPU_OPT_LANCZOS_CLUSTER
+    bool f_dedup = false;
+    long long f_build = -1;
+    int f_probe_D = 0, f_probe_ldm = 0, f_probe_C = 0;  // cached cluster choice for (D, ldm, build)
+    long long f_probe_build = -1;
     // H as a fixed-pattern linear combination of terms (msgpu_upload_hamiltonian_terms):
     // the host copy h_val then holds a generic combination (structure only)
     bool terms = false;
@@ -260,7 +277,7 @@ void msgpu_destroy(msgpu_ctx *c)
     cudaStreamSynchronize(c->stream);
     collect_profile(c);
     DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->qrow, &c->qcolt, &c->qval, &c->qbase,
-                     &c->krow, &c->kcol, &c->kval, &c->bits,
+                     &c->fblk, &c->fval, &c->frow, &c->fdsrc, &c->fdiag, &c->krow, &c->kcol, &c->kval, &c->bits,
                      &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
@@ -291,6 +308,14 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
         if (v < -1 || v >= kNumSpmmVariants || v != value) return fail(c, MSGPU_ERR_INVALID, "SpMM variant out of range");
         c->spmm_variant = v;
         c->q_tile = 0;  // tune again among the allowed variants
+        return MSGPU_OK;
+    }
+    if (key == MSGPU_OPT_LANCZOS_CLUSTER) {
+        const int v = static_cast<int>(value);
+        if (v != value || !(v == -1 || v == 0 || v == 1 || v == 2 || v == 4 || v == 8 || v == 16))
+            return fail(c, MSGPU_ERR_INVALID, "Lanczos cluster size must be -1, 0, 1, 2, 4, 8 or 16");
+        c->f_opt = v;
+        c->f_probe_D = 0;  // choose again
         return MSGPU_OK;
     }
     if (key == MSGPU_OPT_TAYLOR_TOL) {
@@ -1047,6 +1072,10 @@ int build_quartet(msgpu_ctx *c)
     c->q_s1 = s1;
     c->q_s2 = s2;
     c->q_nblocks = nb;
+    ++c->q_build;
+    c->q_hrow = std::move(rowptr);
+    c->q_hblk = std::move(blks);
+    c->q_hval = std::move(vals);
     c->q_tile = 0;
     c->q_nslots = src.size();
     if (c->terms) {
@@ -1065,6 +1094,215 @@ QuartetC quartet_view(const msgpu_ctx *c)
 {
     return QuartetC{static_cast<const int *>(c->qrow.p), static_cast<const int2 *>(c->qcolt.p),
                     static_cast<const float4 *>(c->qval.p), static_cast<const int *>(c->qbase.p)};
+}
+
+// ------------------------------------------------- cluster-resident Lanczos
+// Bound on the off-diagonal blocks one CTA of k_lanczos_fused<C> stages (the
+// quartets' own blocks are counted too).
+int fused_blocks_max(const msgpu_ctx *c, int C)
+{
+    const int Q = c->D / 4, Qc = ceil_div(Q, C);
+    int mx = 0;
+    for (int r = 0; r < C; ++r) {
+        const int qb = std::min(Q, r * Qc), qe = std::min(Q, qb + Qc);
+        mx = std::max(mx, c->q_hrow[qe] - c->q_hrow[qb]);
+    }
+    return mx;
+}
+
+// Descriptors of k_lanczos_fused for cluster size C (Qc = ceil(Q / C)
+// quartets per CTA).  Each quartet's own block is set apart (its type and
+// value offset, expanded to a full 4x4 on the device by k_fused_diag before
+// every launch, so values refreshed in place are followed); the other blocks
+// keep their values and get (owner rank, local quartet) for their neighbour.
+// For a static H, off-diagonal value blocks with equal bits share one copy --
+// the flip blocks of a nucleus repeat over all quartets -- so the values the
+// CTAs read stay in L1.  With Hamiltonian terms the values are refreshed in
+// place every step, so the blocks keep their own slots.
+int build_fused(msgpu_ctx *c, int C)
+{
+    if (c->f_build == c->q_build && c->f_C == C) return MSGPU_OK;
+    const int Q = c->D / 4, Qc = ceil_div(Q, C), s1 = c->s1, s2 = c->s2;
+    const bool dedup = !c->terms;
+    const std::vector<int2> &hb = c->q_hblk;
+    const std::vector<float> &hv = c->q_hval;
+    std::vector<int> frow(Q + 1, 0);
+    std::vector<int2> fb, dsrc(Q, make_int2(-1, 0));
+    fb.reserve(hb.size());
+    std::vector<float> fv;
+    std::map<std::vector<uint32_t>, int> seen;  // value bits -> offset in fv (float4 units)
+    std::vector<int> ord;
+    for (int q = 0; q < Q; ++q) {
+        const int own = (q / (s1 / 2)) * (2 * s1) + ((q / s2) % (s1 / (2 * s2))) * (2 * s2) + q % s2;
+        const int kb = c->q_hrow[q], ke = c->q_hrow[q + 1];
+        // Off-diagonal blocks by |neighbour base - own base|, one flip block per
+        // nucleus in stride order: the lanes of a warp hold neighbouring
+        // quartets, so block k is the same nucleus, type and owner CTA on every
+        // lane (no divergent block types, no split between local and remote
+        // gathers).
+        ord.clear();
+        for (int k = kb; k < ke; ++k) {
+            if ((hb[k].x >> 3) == own)
+                dsrc[q] = make_int2(hb[k].x & 7, hb[k].y);
+            else
+                ord.push_back(k);
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+            const long long dx = (hb[x].x >> 3) - own, dy = (hb[y].x >> 3) - own;
+            return std::llabs(dx) != std::llabs(dy) ? std::llabs(dx) < std::llabs(dy) : dx < dy;
+        });
+        for (int k : ord) {
+            const int b = hb[k].x >> 3, type = hb[k].x & 7;
+            // inverse of quartet_base: drop the two electron digits of the base row
+            const int qn = (b / (2 * s1)) * (s1 / 2) + ((b / (2 * s2)) % (s1 / (2 * s2))) * s2 + b % s2;
+            const int r = qn / Qc, lq = qn - r * Qc;
+            int voff = hb[k].y;
+            if (dedup) {
+                const size_t nf = 4 * static_cast<size_t>(type == 0 ? 8 : type <= 2 ? 4 : 2);
+                const size_t at = 4 * static_cast<size_t>(voff);
+                std::vector<uint32_t> key(nf);
+                std::memcpy(key.data(), hv.data() + at, nf * sizeof(float));
+                auto it = seen.find(key);
+                if (it == seen.end()) {
+                    const int fo = static_cast<int>(fv.size() / 4);
+                    fv.insert(fv.end(), hv.begin() + at, hv.begin() + at + nf);
+                    it = seen.emplace(std::move(key), fo).first;
+                }
+                voff = it->second;
+            }
+            fb.push_back(make_int2((lq << 7) | (r << 3) | type, voff));
+        }
+        frow[q + 1] = static_cast<int>(fb.size());
+    }
+    int rc;
+    cudaError_t e;
+    if ((rc = ensure(c, c->fblk, sizeof(int2) * std::max<size_t>(1, fb.size()), "fused Lanczos blocks")) ||
+        (rc = ensure(c, c->frow, sizeof(int) * (Q + 1), "fused Lanczos row pointers")) ||
+        (rc = ensure(c, c->fdsrc, sizeof(int2) * Q, "fused Lanczos diagonal map")) ||
+        (rc = ensure(c, c->fdiag, sizeof(float4) * 8 * static_cast<size_t>(Q), "fused Lanczos diagonal blocks")))
+        return rc;
+    if ((e = cudaMemcpyAsync(c->fblk.p, fb.data(), sizeof(int2) * fb.size(), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->frow.p, frow.data(), sizeof(int) * (Q + 1), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->fdsrc.p, dsrc.data(), sizeof(int2) * Q, cudaMemcpyHostToDevice, c->stream)))
+        return cuda_fail(c, e, "fused Lanczos blocks");
+    if (dedup) {
+        if ((rc = ensure(c, c->fval, sizeof(float) * std::max<size_t>(4, fv.size()), "fused Lanczos values")))
+            return rc;
+        if ((e = cudaMemcpyAsync(c->fval.p, fv.data(), sizeof(float) * fv.size(), cudaMemcpyHostToDevice, c->stream)))
+            return cuda_fail(c, e, "fused Lanczos values");
+    }
+    if ((e = cudaStreamSynchronize(c->stream))) return cuda_fail(c, e, "fused Lanczos blocks");
+    c->f_C = C;
+    c->f_build = c->q_build;
+    c->f_dedup = dedup;
+    c->f_nblk_max = fused_blocks_max(c, C);
+    return MSGPU_OK;
+}
+
+using FusedFn = void (*)(QuartetF, float2 *, size_t, double *, double *, double *, int *, int, int, int, int, int, int,
+                         int);
+
+FusedFn fused_kernel(int C)
+{
+    switch (C) {
+    case 1: return k_lanczos_fused<1>;
+    case 2: return k_lanczos_fused<2>;
+    case 4: return k_lanczos_fused<4>;
+    case 8: return k_lanczos_fused<8>;
+    case 16: return k_lanczos_fused<16>;
+    default: return nullptr;
+    }
+}
+
+// Allow the kernel the device's opt-in shared memory (each launch still asks
+// for its own size) and, for 16-CTA clusters, the non-portable cluster size.
+cudaError_t fused_prepare(const msgpu_ctx *c, FusedFn fn, int C)
+{
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (!e) e = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (!e && C > 8)
+        e = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+}
+
+cudaLaunchConfig_t fused_config(int C, int ldm, size_t smem, cudaStream_t st, cudaLaunchAttribute *attr)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(C * (ldm / (2 * kFusedPairs))));
+    cfg.blockDim = dim3(kFusedThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Whether k_lanczos_fused<C> runs this shape: a CTA's share of the vectors and
+// of the quartet structure fits its shared memory, and at least one cluster of
+// C such CTAs can be resident on the device.
+bool fused_fits(msgpu_ctx *c, int C)
+{
+    const int Q = c->D / 4, Qc = ceil_div(Q, C);
+    if (Qc > kFusedMaxQc) return false;
+    const FusedFn fn = fused_kernel(C);
+    const size_t smem = fused_smem_bytes(Qc, fused_blocks_max(c, C), C);
+    int optin = 0, nclusters = 0;
+    cudaLaunchAttribute attr[1];
+    const cudaLaunchConfig_t cfg = fused_config(C, c->ldm, smem, c->stream, attr);
+    const bool ok = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) == cudaSuccess &&
+                    smem <= static_cast<size_t>(optin) && fused_prepare(c, fn, C) == cudaSuccess &&
+                    cudaOccupancyMaxActiveClusters(&nclusters, reinterpret_cast<const void *>(fn), &cfg) == cudaSuccess &&
+                    nclusters > 0;
+    cudaGetLastError();  // a refused query is an answer, not an error of the run
+    return ok;
+}
+
+// Cluster size of k_lanczos_fused for the current shape, or 0 for the
+// four-kernel iteration (MSGPU_OPT_LANCZOS_CLUSTER 0, the default, or nothing
+// fits): with -1 the smallest power of two whose CTAs hold their share (unless
+// MSGPU_OPT_SPMM_VARIANT forces an SpMM variant), else the size asked for.
+// Needs the quartet form.
+int fused_cluster(msgpu_ctx *c)
+{
+    if (c->f_opt == 0 || (c->f_opt < 0 && c->spmm_variant >= 0)) return 0;  // a forced SpMM variant keeps its loop
+    if (c->f_probe_D == c->D && c->f_probe_ldm == c->ldm && c->f_probe_build == c->q_build) return c->f_probe_C;
+    int pick = 0;
+    for (int C : {1, 2, 4, 8, 16})
+        if ((c->f_opt < 0 || c->f_opt == C) && fused_fits(c, C)) {
+            pick = C;
+            break;
+        }
+    c->f_probe_D = c->D;
+    c->f_probe_ldm = c->ldm;
+    c->f_probe_build = c->q_build;
+    c->f_probe_C = pick;
+    return pick;
+}
+
+int launch_fused(msgpu_ctx *c, int C, float2 *Wb, size_t n, double *sc, double *td, double *to, int *mdim, int m)
+{
+    if (int rc = build_fused(c, C)) return rc;
+    const int Q = c->D / 4, Qc = ceil_div(Q, C);
+    const size_t smem = fused_smem_bytes(Qc, c->f_nblk_max, C);
+    const QuartetF H{static_cast<const int *>(c->frow.p), static_cast<const int2 *>(c->fblk.p),
+                     static_cast<const float4 *>(c->f_dedup ? c->fval.p : c->qval.p),
+                     static_cast<const float4 *>(c->fdiag.p), static_cast<const int *>(c->qbase.p)};
+    k_fused_diag<<<ceil_div(8 * Q, 256), 256, 0, c->stream>>>(static_cast<const int2 *>(c->fdsrc.p),
+                                                               static_cast<const float2 *>(c->qval.p),
+                                                               static_cast<float4 *>(c->fdiag.p), Q);
+    const FusedFn fn = fused_kernel(C);
+    cudaError_t e = cudaGetLastError();
+    if (!e) e = fused_prepare(c, fn, C);
+    cudaLaunchAttribute attr[1];
+    const cudaLaunchConfig_t cfg = fused_config(C, c->ldm, smem, c->stream, attr);
+    if (!e)
+        e = cudaLaunchKernelEx(&cfg, fn, H, Wb, n, sc, td, to, mdim, Q, Qc, c->f_nblk_max, c->ldm, m, c->s1, c->s2);
+    return e ? cuda_fail(c, e, "fused Lanczos launch") : MSGPU_OK;
 }
 
 // Autotuner for the quartet SpMM: times each candidate tile (quartets per
@@ -1408,11 +1646,14 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 static_cast<double *>(c->qpart_nrm.p));
     }
     yield_update(0.0, 1, 0);
+    int fused_c = 0;  // cluster size of k_lanczos_fused, 0: the four-kernel iteration
     if (prec == MSGPU_PREC_C64) {
         if (int rc = build_quartet(c)) return rc;
-        if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc, static_cast<float2 *>(c->ubuf.p),
-                                       static_cast<double *>(c->part.p)))
-            return rc;
+        fused_c = fused_cluster(c);
+        if (!fused_c)
+            if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc,
+                                           static_cast<float2 *>(c->ubuf.p), static_cast<double *>(c->part.p)))
+                return rc;
     }
 
     const int R = c->rows_per_tile, nt = c->ntiles;
@@ -1602,9 +1843,13 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             double *alpha = static_cast<double *>(c->alpha.p);
             double *td = static_cast<double *>(c->tdiag.p), *to = static_cast<double *>(c->toff.p);
             dim3 grid(nt, ldm / 64);
-            const int QT = c->q_tile, nqt = ceil_div(Q, QT);
+            const int QT = c->q_tile, nqt = ceil_div(Q, std::max(1, QT));
             dim3 qgrid_apply(nqt, ldm / 64);
-            for (int j = 0; j < m; ++j) {
+            if (fused_c) {
+                Timed tm(c, KC_LANCZOS);
+                if (int rc = launch_fused(c, fused_c, Wb, n, sc, td, to, static_cast<int *>(c->mdim.p), m)) return rc;
+            }
+            for (int j = 0; j < (fused_c ? 0 : m); ++j) {
                 {
                     Timed tm(c, KC_APPLY);
                     launch_apply(c, c->q_variant, QT, qgrid_apply, st, Wb + j * n, sc + static_cast<size_t>(j) * ldm, U,
