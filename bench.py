@@ -123,6 +123,11 @@ def _barrier(world: int):
     ranks.barrier(world)
 
 
+# Bounded CPU samples: about 10 s of work each (the oracle's rate per core is
+# fixed, so the trajectory count follows the core count).
+CPU_SAMPLE_STEPS = 128  # precision workload: 2 trajectories per core x 128 steps
+
+
 def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
     """The CPU restatement (complex128 Arnoldi/MGS, per-column Krylov) on a bounded sample."""
     from oracle import density as den
@@ -150,12 +155,12 @@ def run_reference(args):
     from molspin_b200 import systems as S
     w = S.precision_large(M=args.traj, steps=args.chunk)
     threads = os.cpu_count() or 1
-    traj = max(threads, 2 * threads)
+    traj = 2 * threads
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference(w, threads, 1, threads)
     vals = []
     for _ in range(max(1, min(args.steps, 3))):
-        vals.append(cpu_reference(w, traj, 2, threads))
+        vals.append(cpu_reference(w, traj, CPU_SAMPLE_STEPS, threads))
     v = sum(x["value"] for x in vals) / len(vals)
     line = {
         "impl": "reference", "metric": "SSE traj-steps/s (stochastic HSGeneral, Krylov m=20, D=16384)",
@@ -297,7 +302,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cpu = cpu_reference(w, threads, 2, threads)
+        cpu = cpu_reference(w, 2 * threads, CPU_SAMPLE_STEPS, threads)
 
     p.close()
     if rank == 0:
@@ -439,7 +444,7 @@ def run_plain(args):
     launches = p.launch_count() - l0[0]
     e2e = None if args.no_e2e else _e2e(p, world, F, times, w.krylov, "c128", "krylov", max(1, min(args.steps, 3)))
     p.close()
-    cpu = _cpu_port(w, w.M, 500) if rank == 0 and world == 1 and not args.no_cpu else None
+    cpu = _cpu_port(w, w.M, w.steps) if rank == 0 and world == 1 and not args.no_cpu else None  # the whole workload
     _emit(rank, {
         "metric": "SSE traj-steps/s (plain complex128, D=64, m=16)", "value": world * w.M * chunk * args.steps / (el / 1e3),
         "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -511,7 +516,7 @@ def run_dense(args):
     e2e = None if args.no_e2e else _e2e(p, world, F, times, w.krylov, prec, "dense", max(1, min(args.steps, 3)))
     p.close()
     # the reference has no dense propagator: its CPU path is the Krylov step
-    cpu = _cpu_port(w, 64, 20) if rank == 0 and world == 1 and not args.no_cpu else None
+    cpu = _cpu_port(w, 8 * (os.cpu_count() or 1), 600) if rank == 0 and world == 1 and not args.no_cpu else None
     _emit(rank, {
         "metric": "SSE traj-steps/s (dense tensor-core propagator, D=1024)",
         "value": world * M * chunk * args.steps / (el / 1e3), "unit": "traj-steps/s", "n_gpus": world,
