@@ -252,6 +252,11 @@ def run_ours(args):
     traffic = 243.9e6 if (D, M) == (16384, 1024) else None
     apply_avg_s = apply_ms / max(1, apply_n) / 1e3
     achieved = alg_bytes / apply_avg_s / 1e9 if apply_n else None
+    # the whole time step against HBM: m SpMMs, m-1 updates (4 vectors each) and
+    # the combine ((m + 2) vectors); expm, reductions and yields are negligible
+    m_k = w.krylov
+    step_bytes = m_k * alg_bytes + (m_k - 1) * 4 * D * M * 8 + (m_k + 2) * D * M * 8
+    step_s = el_max / 1e3 / (K * chunk)
 
     # plain complex128 path (reference-faithful Arnoldi) on a short segment,
     # and the singlet-yield deviation of the complex64 form from it
@@ -321,6 +326,9 @@ def run_ours(args):
                          "avg_launch_ms": apply_avg_s * 1e3, "launches_timed": apply_n,
                          "timing": "CUDA events around every launch of every 8th time step (sampled)",
                          "share_of_step": apply_avg_s * 1e3 * w.krylov * chunk * K / el_ms if el_ms else None},
+            "step_roofline": {"bound": "hbm", "alg_bytes_per_time_step": step_bytes, "time_step_ms": step_s * 1e3,
+                              "achieved": step_bytes / step_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                              "frac": step_bytes / step_s / 1e9 / hbm_peak, "peak_kind": peak_kind},
             "kernel_avg_ms": {"apply": apply_ms / max(1, apply_n), "update": orth_ms / max(1, orth_n),
                               "combine": comb_ms / max(1, comb_n),
                               **({"lanczos_cluster_resident": fused_ms / fused_n} if fused_n else {})},
