@@ -127,6 +127,11 @@ def _barrier(world: int):
 # fixed, so the trajectory count follows the core count).
 CPU_SAMPLE_STEPS = 128  # precision workload: 2 trajectories per core x 128 steps
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one SpMM launch
+# from an ncu capture, by (D, trajectories per launch): 1024 trajectories, one
+# group: 138.4 MB + 105.5 MB
+TRAFFIC_SPMM = {(16384, 1024): 243.9e6}
+
 
 def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
     """The CPU restatement (complex128 Arnoldi/MGS, per-column Krylov) on a bounded sample."""
@@ -206,6 +211,7 @@ def run_ours(args):
     p.set_electron_pair(*sysm.electron_strides())
     p.set_observables(obs)
     p.set_factors(F)
+    groups = int(p.get_option(L.OPT_TRAJ_GROUPS))  # trajectory groups of the step (one SpMM launch each)
 
     def bench_step(first: bool, k: int):
         p.propagate(times, w.krylov, "c64", step_offset=k * chunk, accumulate=not first)
@@ -246,16 +252,15 @@ def run_ours(args):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
-    alg_bytes = 2 * D * M * 8 + len(col) * 12 + 4 * (D + 1)
-    # DRAM bytes per launch of this kernel at this workload (dram__bytes_read.sum
-    # + dram__bytes_write.sum of one ncu capture: 138.4 MB + 105.5 MB)
-    traffic = 243.9e6 if (D, M) == (16384, 1024) else None
+    width = M // groups  # trajectories of one SpMM launch
+    alg_bytes = 2 * D * width * 8 + len(col) * 12 + 4 * (D + 1)
+    traffic = TRAFFIC_SPMM.get((D, width))
     apply_avg_s = apply_ms / max(1, apply_n) / 1e3
     achieved = alg_bytes / apply_avg_s / 1e9 if apply_n else None
     # the whole time step against HBM: m SpMMs, m-1 updates (4 vectors each) and
     # the combine ((m + 2) vectors); expm, reductions and yields are negligible
     m_k = w.krylov
-    step_bytes = m_k * alg_bytes + (m_k - 1) * 4 * D * M * 8 + (m_k + 2) * D * M * 8
+    step_bytes = m_k * groups * alg_bytes + (m_k - 1) * 4 * D * M * 8 + (m_k + 2) * D * M * 8
     step_s = el_max / 1e3 / (K * chunk)
 
     # plain complex128 path (reference-faithful Arnoldi) on a short segment,
@@ -318,14 +323,15 @@ def run_ours(args):
             "dtype": "c64 (FP64 reductions/expm/sums)", "data": "synthetic (seeded)",
             "config": {"workload": w.name, "trajectories_per_gpu": M, "dim": D, "nnz": int(len(col)),
                        "krylov": w.krylov, "dt_ns": w.dt, "time_steps_per_bench_step": chunk,
-                       "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos",
+                       "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos", "trajectory_groups": groups,
                        "parallelism": f"independent trajectory blocks x{world}"},
             "roofline": {"bound": "hbm", "kernel": "quartet SpMM (k_lanczos_apply_*, autotuned variant)", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": traffic,
                          "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": apply_avg_s * 1e3, "launches_timed": apply_n,
                          "timing": "CUDA events around every launch of every 8th time step (sampled)",
-                         "share_of_step": apply_avg_s * 1e3 * w.krylov * chunk * K / el_ms if el_ms else None},
+                         "share_of_step": apply_avg_s * 1e3 * w.krylov * groups * chunk * K / el_ms if el_ms else None,
+                         "trajectories_per_launch": width},
             "step_roofline": {"bound": "hbm", "alg_bytes_per_time_step": step_bytes, "time_step_ms": step_s * 1e3,
                               "achieved": step_bytes / step_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                               "frac": step_bytes / step_s / 1e9 / hbm_peak, "peak_kind": peak_kind},

@@ -97,6 +97,13 @@ extern "C" {
                                         Same results to FP32 rounding; at D=16384 with 1024
                                         trajectories on a B200 it is the slower of the two
                                         (latency-bound at one 512-thread CTA per SM) */
+#define MSGPU_OPT_TRAJ_GROUPS 5       /* complex64 streamed form: 0 (default) splits a block of
+                                        512 or more trajectories into 2 groups whose step
+                                        sequences run on two streams, so that one group's SpMM
+                                        (held by the SM's load pipe) overlaps the other's
+                                        memory-bound update and combine; 1: one group; 2 or 4:
+                                        that many groups when each is a multiple of 128
+                                        trajectories.  Results do not depend on it. */
 
 /* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
  * dimensions (the whole time loop in one launch, one warp per trajectory,
@@ -224,6 +231,9 @@ int msgpu_set_form(msgpu_ctx *ctx, int form);
 
 /* Set an option (MSGPU_OPT_*). */
 int msgpu_set_option(msgpu_ctx *ctx, int key, double value);
+/* Read an option back; for MSGPU_OPT_TRAJ_GROUPS the number of groups the
+ * current trajectory block runs in (once factors are uploaded). */
+int msgpu_get_option(msgpu_ctx *ctx, int key, double *value);
 
 /* ---------------------------------------------------------------- batching
  * Many spin systems of uneven dimension and trajectory count propagated by

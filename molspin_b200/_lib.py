@@ -35,6 +35,7 @@ PROP_RK4 = 3
 OPT_TAYLOR_TOL = 2
 OPT_SPMM_VARIANT = 3
 OPT_LANCZOS_CLUSTER = 4
+OPT_TRAJ_GROUPS = 5
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
 OPT_DENSE_RENORMALIZE = 1
@@ -100,6 +101,7 @@ def _load() -> C.CDLL:
         "msgpu_launch_count": (C.c_longlong, [P]),
         "msgpu_set_form": (I, [P, I]),
         "msgpu_set_option": (I, [P, I, D]),
+        "msgpu_get_option": (I, [P, I, pD]),
         "msgpu_batch_create": (P, [I, C.c_size_t]),
         "msgpu_batch_destroy": (None, [P]),
         "msgpu_batch_last_error": (C.c_char_p, [P]),

@@ -63,6 +63,11 @@ struct msgpu_ctx {
     long long f_build = -1;
     int f_probe_D = 0, f_probe_ldm = 0, f_probe_C = 0;  // cached cluster choice for (D, ldm, build)
     long long f_probe_build = -1;
+    // complex64 streamed step in trajectory groups (MSGPU_OPT_TRAJ_GROUPS): one
+    // group's SpMM overlaps the other's update and combine on a second stream
+    int tgroups_opt = 0;  // 0 auto, else the number of groups asked for
+    cudaStream_t gside = nullptr;
+    cudaEvent_t gfork = nullptr, gjoin = nullptr;
     // H as a fixed-pattern linear combination of terms (msgpu_upload_hamiltonian_terms):
     // the host copy h_val then holds a generic combination (structure only)
     bool terms = false;
@@ -183,9 +188,10 @@ constexpr int kProfileEvery = 8;
 struct Timed {
     msgpu_ctx *c;
     int cls;
+    cudaStream_t s;
     bool on = false;
     cudaEvent_t a = nullptr, b = nullptr;
-    Timed(msgpu_ctx *c_, int cls_) : c(c_), cls(cls_)
+    Timed(msgpu_ctx *c_, int cls_, cudaStream_t s_ = nullptr) : c(c_), cls(cls_), s(s_ ? s_ : c_->stream)
     {
         ++c->launches;
         if (c->prof == 1) {
@@ -196,12 +202,12 @@ struct Timed {
         if (!on) return;
         cudaEventCreate(&a);
         cudaEventCreate(&b);
-        cudaEventRecord(a, c->stream);
+        cudaEventRecord(a, s);
     }
     ~Timed()
     {
         if (!on) return;
-        cudaEventRecord(b, c->stream);
+        cudaEventRecord(b, s);
         c->ev.push_back({cls, {a, b}});
     }
 };
@@ -220,6 +226,17 @@ void collect_profile(msgpu_ctx *c)
 }
 
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+// Trajectory groups of the complex64 streamed step (MSGPU_OPT_TRAJ_GROUPS).
+// Each group is a multiple of 128 trajectories, the width of the widest SpMM
+// variant's CTA; auto takes two groups from 512 trajectories up.
+int traj_groups(const msgpu_ctx *c)
+{
+    const int want = c->tgroups_opt > 0 ? c->tgroups_opt : (c->ldm >= 512 ? 2 : 1);
+    for (int g = want; g > 1; g /= 2)
+        if (c->ldm % (128 * g) == 0) return g;
+    return 1;
+}
 
 // Rows per tile: keep about 64-128 row tiles per trajectory tile so that the
 // partial-sum buffers stay small and every SM has several CTAs.
@@ -285,6 +302,9 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->dense_part, &c->hterms, &c->qsrc};
     for (DevBuf *b : all) release(c, *b);
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
+    if (c->gfork) cudaEventDestroy(c->gfork);
+    if (c->gjoin) cudaEventDestroy(c->gjoin);
+    if (c->gside) cudaStreamDestroy(c->gside);
     for (auto &a : c->dense_allocs) cudaFree(a.first);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -310,6 +330,14 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
         c->q_tile = 0;  // tune again among the allowed variants
         return MSGPU_OK;
     }
+    if (key == MSGPU_OPT_TRAJ_GROUPS) {
+        const int v = static_cast<int>(value);
+        if (v != value || !(v == 0 || v == 1 || v == 2 || v == 4))
+            return fail(c, MSGPU_ERR_INVALID, "trajectory groups must be 0 (auto), 1, 2 or 4");
+        c->tgroups_opt = v;
+        c->q_tile = 0;  // the variants that fit depend on a group's width
+        return MSGPU_OK;
+    }
     if (key == MSGPU_OPT_LANCZOS_CLUSTER) {
         const int v = static_cast<int>(value);
         if (v != value || !(v == -1 || v == 0 || v == 1 || v == 2 || v == 4 || v == 8 || v == 16))
@@ -324,6 +352,19 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
         return MSGPU_OK;
     }
     return fail(c, MSGPU_ERR_INVALID, "unknown option");
+}
+
+int msgpu_get_option(msgpu_ctx *c, int key, double *value)
+{
+    if (!c || !value) return MSGPU_ERR_INVALID;
+    switch (key) {
+    case MSGPU_OPT_DENSE_RENORMALIZE: *value = c->dense_renorm; return MSGPU_OK;
+    case MSGPU_OPT_TAYLOR_TOL: *value = c->taylor_tol; return MSGPU_OK;
+    case MSGPU_OPT_SPMM_VARIANT: *value = c->spmm_variant; return MSGPU_OK;
+    case MSGPU_OPT_LANCZOS_CLUSTER: *value = c->f_opt; return MSGPU_OK;
+    case MSGPU_OPT_TRAJ_GROUPS: *value = c->ldm ? traj_groups(c) : c->tgroups_opt; return MSGPU_OK;
+    default: return fail(c, MSGPU_ERR_INVALID, "unknown option");
+    }
 }
 
 int msgpu_set_form(msgpu_ctx *c, int form)
@@ -1332,7 +1373,9 @@ constexpr int kCubeMaxQT = 64;  // 128 KB of shared memory
 bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 {
     *smem = 0;
-    if (c->ldm % (64 * kApplyVariants[v].np) != 0) return false;
+    // the step launches it over one trajectory group, the tuner over the whole block
+    if ((c->ldm / traj_groups(c)) % (64 * kApplyVariants[v].np) != 0 || c->ldm % (64 * kApplyVariants[v].np) != 0)
+        return false;
     if (!kApplyVariants[v].cube) return true;
     // the tile's quartet bases must be contiguous: QT divides the second stride
     if (qt > kCubeMaxQT || c->s2 % qt != 0) return false;
@@ -1340,12 +1383,13 @@ bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
     return true;
 }
 
+// width: trajectories of the launch (the pointers start at its first one)
 void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st, const float2 *w, const double *s,
-                  float2 *U, double *part)
+                  float2 *U, double *part, int width)
 {
     size_t smem = 0;
     apply_fits(c, v, qt, &smem);
-    grid.y = c->ldm / (64 * kApplyVariants[v].np);
+    grid.y = width / (64 * kApplyVariants[v].np);
     if (smem) cudaFuncSetAttribute(kApplyVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     kApplyVariants[v].fn<<<grid, kThreads, smem, st>>>(quartet_view(c), w, s, U, part, c->D / 4, c->s1, c->s2, c->ldm,
                                                        qt);
@@ -1375,9 +1419,13 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
         for (size_t k = 0; k < cands.size(); ++k) {
             const int v = cands[k].first, qt = cands[k].second;
             dim3 grid(ceil_div(Q, qt), c->ldm / 64);
-            launch_apply(c, v, qt, grid, c->stream, w, s, U, part);
+            // timed over the whole block, not one group: the step overlaps the
+            // groups, and the tile chosen this way measured faster there (179k
+            // against 175k traj-steps/s at D=16384, 2 x 512 trajectories) although
+            // alone it is the slower one at a group's width (90 against 86 us)
+            launch_apply(c, v, qt, grid, c->stream, w, s, U, part, c->ldm);
             cudaEventRecord(a, c->stream);
-            for (int rep = 0; rep < 2; ++rep) launch_apply(c, v, qt, grid, c->stream, w, s, U, part);
+            for (int rep = 0; rep < 2; ++rep) launch_apply(c, v, qt, grid, c->stream, w, s, U, part, c->ldm);
             cudaEventRecord(b, c->stream);
             cudaEventSynchronize(b);
             float ms = 0.f;
@@ -1842,51 +1890,78 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             double *part = static_cast<double *>(c->part.p);
             double *alpha = static_cast<double *>(c->alpha.p);
             double *td = static_cast<double *>(c->tdiag.p), *to = static_cast<double *>(c->toff.p);
-            dim3 grid(nt, ldm / 64);
+            int *mdim = static_cast<int *>(c->mdim.p);
+            double2 *coef = static_cast<double2 *>(c->coef.p);
+            double *qobs = static_cast<double *>(c->qpart_obs.p), *qnrm = static_cast<double *>(c->qpart_nrm.p);
             const int QT = c->q_tile, nqt = ceil_div(Q, std::max(1, QT));
-            dim3 qgrid_apply(nqt, ldm / 64);
             if (fused_c) {
                 Timed tm(c, KC_LANCZOS);
-                if (int rc = launch_fused(c, fused_c, Wb, n, sc, td, to, static_cast<int *>(c->mdim.p), m)) return rc;
+                if (int rc = launch_fused(c, fused_c, Wb, n, sc, td, to, mdim, m)) return rc;
             }
-            for (int j = 0; j < (fused_c ? 0 : m); ++j) {
-                {
-                    Timed tm(c, KC_APPLY);
-                    launch_apply(c, c->q_variant, QT, qgrid_apply, st, Wb + j * n, sc + static_cast<size_t>(j) * ldm, U,
-                                 part);
+            // Trajectory groups: every kernel below works on columns [t0, t0 + width)
+            // through offset pointers with the row stride ldm, so the groups share
+            // the buffers. With overlap, odd groups run on the second stream and
+            // one group's SpMM runs beside another's update and combine; profiled
+            // steps run the groups back to back so that each launch is timed alone.
+            const int G = fused_c ? 1 : traj_groups(c), width = ldm / G;
+            const bool timed_step = c->prof == 1 || (c->prof == 2 && c->prof_tick % kProfileEvery == 0);
+            const bool overlap = G > 1 && !timed_step;
+            if (overlap) {
+                if (!c->gside && ((e = cudaStreamCreateWithFlags(&c->gside, cudaStreamNonBlocking)) ||
+                                  (e = cudaEventCreateWithFlags(&c->gfork, cudaEventDisableTiming)) ||
+                                  (e = cudaEventCreateWithFlags(&c->gjoin, cudaEventDisableTiming))))
+                    return cuda_fail(c, e, "trajectory group stream");
+                if ((e = cudaEventRecord(c->gfork, st)) || (e = cudaStreamWaitEvent(c->gside, c->gfork, 0)))
+                    return cuda_fail(c, e, "trajectory group fork");
+            }
+            for (int gi = 0; gi < G; ++gi) {
+                const int t0 = gi * width;
+                const size_t tm0 = static_cast<size_t>(t0) * mws;  // offset into the [t][m] T arrays
+                cudaStream_t gs = (overlap && (gi & 1)) ? c->gside : st;
+                dim3 grid(nt, width / 64);
+                for (int j = 0; j < (fused_c ? 0 : m); ++j) {
+                    {
+                        Timed tm(c, KC_APPLY, gs);
+                        launch_apply(c, c->q_variant, QT, dim3(nqt), gs, Wb + j * n + t0,
+                                     sc + static_cast<size_t>(j) * ldm + t0, U + t0, part + t0, width);
+                    }
+                    {
+                        Timed tm(c, KC_REDUCE, gs);
+                        k_lanczos_reduce<<<width / 32, dim3(32, 8), 0, gs>>>(part + t0, nqt, ldm, 0, j, mws, alpha + t0,
+                                                                             td + tm0, to + tm0, mdim + t0);
+                    }
+                    if (j == m - 1) break;  // T_m is complete; w_m is never used
+                    {
+                        Timed tm(c, KC_ORTH, gs);
+                        k_lanczos_update<<<grid, kThreads, 0, gs>>>(
+                            U + t0, Wb + j * n + t0, j > 0 ? Wb + (j - 1) * n + t0 : nullptr,
+                            sc + static_cast<size_t>(j) * ldm + t0, j > 0 ? sc + static_cast<size_t>(j - 1) * ldm + t0 : nullptr,
+                            alpha + t0, Wb + (j + 1) * n + t0, part + t0, D, ldm, R);
+                    }
+                    {
+                        Timed tm(c, KC_REDUCE, gs);
+                        k_lanczos_reduce<<<width / 32, dim3(32, 8), 0, gs>>>(part + t0, nt, ldm, 1, j, mws,
+                                                                             sc + static_cast<size_t>(j + 1) * ldm + t0,
+                                                                             td + tm0, to + tm0, mdim + t0);
+                    }
                 }
                 {
-                    Timed tm(c, KC_REDUCE);
-                    k_lanczos_reduce<<<ldm / 32, dim3(32, 8), 0, st>>>(part, nqt, ldm, 0, j, mws, alpha, td, to,
-                                                                         static_cast<int *>(c->mdim.p));
-                }
-                if (j == m - 1) break;  // T_m is complete; w_m is never used
-                {
-                    Timed tm(c, KC_ORTH);
-                    k_lanczos_update<<<grid, kThreads, 0, st>>>(
-                        U, Wb + j * n, j > 0 ? Wb + (j - 1) * n : nullptr, sc + static_cast<size_t>(j) * ldm,
-                        j > 0 ? sc + static_cast<size_t>(j - 1) * ldm : nullptr, alpha, Wb + (j + 1) * n, part, D, ldm, R);
+                    Timed tm(c, KC_EXPM, gs);
+                    k_lanczos_expm<<<ceil_div(width, 8), 256, 0, gs>>>(
+                        td + tm0, to + tm0, kappa, mdim + t0, beta0 + t0, sc + t0, mws, ldm,
+                        std::max(0, std::min(M - t0, width)), dt, coef + t0, static_cast<int *>(c->status.p));
                 }
                 {
-                    Timed tm(c, KC_REDUCE);
-                    k_lanczos_reduce<<<ldm / 32, dim3(32, 8), 0, st>>>(part, nt, ldm, 1, j, mws,
-                                                                         sc + static_cast<size_t>(j + 1) * ldm, td, to,
-                                                                         static_cast<int *>(c->mdim.p));
+                    Timed tm(c, KC_COMBINE, gs);
+                    Noise gnz = nz;
+                    gnz.traj_offset = static_cast<uint32_t>(t0);
+                    k_combine_pp<true><<<dim3(qt, width / 64), qblock, 0, gs>>>(
+                        Wb + t0, Wb + t0, n, coef + t0, mdim + t0, c->s1, c->s2, Q, ldm, QR, gnz, g, 1, pstep(s),
+                        s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, qobs + t0, qnrm + t0);
                 }
             }
-            {
-                Timed tm(c, KC_EXPM);
-                k_lanczos_expm<<<ceil_div(ldm, 8), 256, 0, st>>>(td, to, kappa, static_cast<int *>(c->mdim.p), beta0,
-                                                                sc, mws, ldm, M, dt, static_cast<double2 *>(c->coef.p),
-                                                                static_cast<int *>(c->status.p));
-            }
-            {
-                Timed tm(c, KC_COMBINE);
-                k_combine_pp<true><<<dim3(qt, ldm / 64), qblock, 0, st>>>(
-                    Wb, Wb, n, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->mdim.p), c->s1, c->s2, Q, ldm,
-                    QR, nz, g, 1, pstep(s), s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po,
-                    static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p));
-            }
+            if (overlap && ((e = cudaEventRecord(c->gjoin, c->gside)) || (e = cudaStreamWaitEvent(st, c->gjoin, 0))))
+                return cuda_fail(c, e, "trajectory group join");
         }
         yield_update(dt, 0, s + 1);
         if ((e = cudaGetLastError())) return cuda_fail(c, e, "step launch");

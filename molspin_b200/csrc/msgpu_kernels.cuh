@@ -884,7 +884,7 @@ struct Noise {
     long long bits_steps;    // number of steps covered by bits
     int M;                   // trajectories in the bit layout
     uint64_t seed;           // philox
-    uint32_t traj_offset;    // philox trajectory id offset
+    uint32_t traj_offset;    // added to the launch's trajectory index (a trajectory group's first)
     double p_full;           // flip probability for a half step of the current step
 };
 
@@ -892,8 +892,9 @@ __device__ __forceinline__ int noise_bit(const Noise &nz, int t, long long step,
 {
     if (step < 0) return 0;
     if (nz.mode == 1) {
-        if (t >= nz.M || step < 0 || step >= nz.bits_steps) return 0;
-        const long long bit = (step * 2 + half) * nz.M + t;
+        const int ta = t + static_cast<int>(nz.traj_offset);  // trajectory in the bit layout
+        if (ta >= nz.M || step < 0 || step >= nz.bits_steps) return 0;
+        const long long bit = (step * 2 + half) * nz.M + ta;
         return (nz.bits[bit >> 3] >> (bit & 7)) & 1;
     }
     if (nz.mode == 2)

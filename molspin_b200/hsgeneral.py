@@ -204,6 +204,11 @@ class HSPropagatorB200:
     def set_option(self, key: int, value: float):
         _check(self.ctx, L.lib.msgpu_set_option(self.ctx, int(key), float(value)))
 
+    def get_option(self, key: int) -> float:
+        v = C.c_double(0.0)
+        _check(self.ctx, L.lib.msgpu_get_option(self.ctx, int(key), C.byref(v)))
+        return v.value
+
     def set_form(self, form: str | int):
         """"auto" | "streamed" | "resident" (see MSGPU_FORM_* in include/msgpu.h)."""
         codes = {"auto": L.FORM_AUTO, "streamed": L.FORM_STREAMED, "resident": L.FORM_RESIDENT}

@@ -122,3 +122,38 @@ def test_option_values():
         for v in (3, 32, -2, 1.5):
             with pytest.raises(hs.MsgpuError):
                 p.set_option(L.OPT_LANCZOS_CLUSTER, v)
+
+
+@pytest.mark.parametrize("noise_mode", ["philox", "replay"])
+def test_trajectory_groups_do_not_change_results(noise_mode):
+    # MSGPU_OPT_TRAJ_GROUPS: the block in 1, 2 or 4 groups (the second on its
+    # own stream) gives bitwise the same yields and values; 1000 trajectories
+    # leave the last group partly padded
+    system = h.random_system([2] * 5, [2] * 3, seed=72, aniso=True, st_rate=0.06)
+    M, times = 1000, S.time_grid(12.0, 1.0)
+    F = system.trace_samples(M, 2.5)
+    if noise_mode == "philox":
+        noise = (system.st_rate, L.NOISE_PHILOX, 17)
+    else:
+        bits = hs.reference_flip_bits(2.5, system.st_rate, times, M, 0)
+        noise = (system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M)
+    out = {}
+    for groups in (1, 2, 4):
+        with hs.HSPropagatorB200(0) as p:
+            p.set_form("streamed")
+            p.set_option(L.OPT_TRAJ_GROUPS, groups)
+            p.set_hamiltonian(*system.hamiltonian_csr())
+            p.set_reaction(kappa=system.kappa())
+            p.set_electron_pair(*system.electron_strides())
+            p.set_observables([(op, rate) for _, op, rate in system.observables()])
+            p.set_noise(*noise)
+            p.set_factors(F)
+            p.propagate(times, 12, "c64")
+            assert p.get_option(L.OPT_TRAJ_GROUPS) == groups
+            out[groups] = (p.yields()[0], p.values(), p.get_factors())
+    for groups in (2, 4):
+        for a, b in zip(out[groups], out[1]):
+            np.testing.assert_array_equal(a, b)
+    with hs.HSPropagatorB200(0) as p:
+        with pytest.raises(hs.MsgpuError):
+            p.set_option(L.OPT_TRAJ_GROUPS, 3)
