@@ -128,9 +128,9 @@ def _barrier(world: int):
 CPU_SAMPLE_STEPS = 128  # precision workload: 2 trajectories per core x 128 steps
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one SpMM launch
-# from an ncu capture, by (D, trajectories per launch): 1024 trajectories, one
-# group: 138.4 MB + 105.5 MB
-TRAFFIC_SPMM = {(16384, 1024): 243.9e6}
+# from an ncu capture, by (D, trajectories per launch): 1024 trajectories (one
+# group): 138.4 MB + 105.5 MB; 512 (one of two groups): 73.9 MB + 43.6 MB
+TRAFFIC_SPMM = {(16384, 1024): 243.9e6, (16384, 512): 117.5e6}
 
 
 def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
