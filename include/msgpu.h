@@ -217,10 +217,11 @@ int msgpu_fetch_values(msgpu_ctx *ctx, double *values);
  * 0 apply (SpMM), 1 orth/update, 2 reductions, 3 expm, 4 combine, 5 yield,
  * 6 dense GEMM (tensor cores), 7 cluster-resident Lanczos recurrence (one
  * launch per step, MSGPU_OPT_LANCZOS_CLUSTER).  enable: 0 off; 1 every launch; 2 sampled --
- * every launch of every 8th time step of the streamed step loop, and every
- * 8th dense GEMM (events between kernels cost them their overlap, so timing
- * every launch slows a many-launch step by about 10 %; the sampled mode
- * costs about 1 %).  msgpu_profile_read returns the total time and the
+ * every launch of every 32nd time step of the streamed step loop (whose
+ * trajectory groups then run back to back, so each launch is timed alone),
+ * and every 8th dense GEMM (events between kernels cost them their overlap,
+ * so timing every launch slows a many-launch step by 10 % or more; the
+ * sampled mode costs about 1 %).  msgpu_profile_read returns the total time and the
  * number of launches that time covers. */
 int msgpu_profile_enable(msgpu_ctx *ctx, int enable);
 int msgpu_profile_read(msgpu_ctx *ctx, int kernel_class, double *total_ms, long long *launches);

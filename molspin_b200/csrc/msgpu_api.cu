@@ -125,6 +125,7 @@ struct msgpu_ctx {
     int prof = 0;                   // 0 off, 1 every launch, 2 sampled (see msgpu_profile_enable)
     long long prof_tick = -1;       // time step being issued (-1 outside the step loop)
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+    std::vector<cudaEvent_t> evpool;  // recycled timing events (creating two per timed launch stalls the host)
     double prof_ms[KC_N] = {0};
     long long prof_n[KC_N] = {0};
 };
@@ -178,12 +179,15 @@ int device_guard(msgpu_ctx *c)
     return MSGPU_OK;
 }
 
-// Sampled profiling times every launch of every kProfileEvery-th time step:
-// an event between two kernels costs them their overlap, so timing every
-// launch of every step slows a many-launch step by about 10 %, and timing
-// one step in kProfileEvery about 1 %.  (The first launch of a class in a
-// step is not representative: the first SpMM after the combine runs slower.)
-constexpr int kProfileEvery = 8;
+// Sampled profiling times every launch of every kProfileEvery-th time step
+// of the streamed loop: an event between two kernels costs them their
+// overlap, and a timed step also runs its trajectory groups back to back, so
+// timing every launch slows the step by 10 % or more; one step in 32 costs
+// about 1 %.  (The first launch of a class in a step is not representative:
+// the first SpMM after the combine runs slower.)  The dense form times every
+// kProfileEveryDense-th GEMM.
+constexpr int kProfileEvery = 32;
+constexpr int kProfileEveryDense = 8;
 
 struct Timed {
     msgpu_ctx *c;
@@ -200,9 +204,20 @@ struct Timed {
             on = true;
         }
         if (!on) return;
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
+        a = take();
+        b = take();
         cudaEventRecord(a, s);
+    }
+    cudaEvent_t take()
+    {
+        cudaEvent_t e = nullptr;
+        if (!c->evpool.empty()) {
+            e = c->evpool.back();
+            c->evpool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
     }
     ~Timed()
     {
@@ -219,8 +234,8 @@ void collect_profile(msgpu_ctx *c)
         cudaEventElapsedTime(&ms, e.second.first, e.second.second);
         c->prof_ms[e.first] += ms;
         c->prof_n[e.first] += 1;
-        cudaEventDestroy(e.second.first);
-        cudaEventDestroy(e.second.second);
+        c->evpool.push_back(e.second.first);
+        c->evpool.push_back(e.second.second);
     }
     c->ev.clear();
 }
@@ -302,6 +317,7 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->dense_part, &c->hterms, &c->qsrc};
     for (DevBuf *b : all) release(c, *b);
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
+    for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
     if (c->gfork) cudaEventDestroy(c->gfork);
     if (c->gjoin) cudaEventDestroy(c->gjoin);
     if (c->gside) cudaStreamDestroy(c->gside);
@@ -819,7 +835,7 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
     long long gemm_n = 0;
     c->launches += 2LL * (p->ntimes - 1) + 4;  // GEMM + epilogue per step; first epilogue, last values, two layout copies
     if ((rc = msgpu::dense_run(c->dense, run, c->psi128.p, ldm, st, err, c->prof ? &gemm_ms : nullptr, &gemm_n,
-                               c->prof == 2 ? kProfileEvery : 1)))
+                               c->prof == 2 ? kProfileEveryDense : 1)))
         return fail(c, rc, err);
     if (c->prof) {
         c->prof_ms[KC_GEMM] += gemm_ms;

@@ -218,7 +218,7 @@ class HSPropagatorB200:
         return int(L.lib.msgpu_launch_count(self.ctx))
 
     def profile(self, enable: bool | int = True):
-        """True/1: time every launch; 2: sampled (every 8th time step); False/0: off."""
+        """True/1: time every launch; 2: sampled (every 32nd time step, every 8th dense GEMM); False/0: off."""
         mode = int(enable) if not isinstance(enable, bool) else (1 if enable else 0)
         _check(self.ctx, L.lib.msgpu_profile_enable(self.ctx, mode))
 
