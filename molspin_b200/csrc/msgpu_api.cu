@@ -1687,11 +1687,14 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     double *beta0 = static_cast<double *>(c->beta0.p);
     auto yield_update = [&](double dt, int init, int row) {
         Timed tm(c, KC_YIELD);
-        k_yield_update<<<1, 1024, 0, st>>>(static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p),
-                                           qt, nobs, ldm, M, static_cast<double *>(c->rates_d.p), dt, init,
-                                           static_cast<double *>(c->prev.p), static_cast<double *>(c->acc.p),
-                                           static_cast<double *>(c->comp.p), beta0, sc, values + static_cast<size_t>(row) * nobs,
-                                           static_cast<int *>(c->status.p));
+        ++c->launches;  // two kernels: per trajectory, then the ensemble value
+        k_yield_traj<<<dim3(ceil_div(ldm, 128), nobs + 1), 128, 0, st>>>(
+            static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p), qt, nobs, ldm,
+            static_cast<double *>(c->rates_d.p), dt, init, static_cast<double *>(c->prev.p),
+            static_cast<double *>(c->acc.p), static_cast<double *>(c->comp.p), beta0, sc,
+            static_cast<int *>(c->status.p));
+        k_yield_values<<<1, 1024, 0, st>>>(static_cast<double *>(c->prev.p), nobs, ldm, M,
+                                           values + static_cast<size_t>(row) * nobs);
     };
 
     // Evaluate the first time point and apply the first half-step flip.

@@ -1155,6 +1155,72 @@ __global__ void k_yield_update(const double *__restrict__ part_obs, const double
     }
 }
 
+// The per-trajectory part of k_yield_update spread over the GPU: thread t of
+// grid row o sums the tile partials of observable o (o == nobs: the squared
+// norm) in tile order, exactly as k_yield_update does, so the results are the
+// same bits.  One 1024-thread CTA reads 5 x 64 partials per thread serially
+// and took about 120 us per time step at 1024 trajectories; this form takes a
+// few microseconds.  Grid (ceil(ldm / 128), nobs + 1), 128 threads.
+__global__ void __launch_bounds__(128)
+k_yield_traj(const double *__restrict__ part_obs, const double *__restrict__ part_nrm, int ntiles, int nobs, int ldm,
+             const double *__restrict__ rates, double dt, int init, double *__restrict__ prev,
+             double *__restrict__ acc, double *__restrict__ comp, double *__restrict__ beta0,
+             double *__restrict__ inv0, int *__restrict__ status)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = blockIdx.y;
+    if (t >= ldm) return;
+    bool bad = false;
+    if (o < nobs) {
+        double v = 0.0;
+#pragma unroll 8
+        for (int tile = 0; tile < ntiles; ++tile) v += part_obs[(static_cast<size_t>(tile) * nobs + o) * ldm + t];
+        v *= rates[o];
+        const size_t k = static_cast<size_t>(o) * ldm + t;
+        if (!init) {
+            const double term = 0.5 * dt * (prev[k] + v) - comp[k];
+            const double s = acc[k] + term;
+            comp[k] = (s - acc[k]) - term;
+            acc[k] = s;
+        }
+        prev[k] = v;
+        if (!isfinite(v)) bad = true;
+    } else {
+        double nn = 0.0;
+#pragma unroll 8
+        for (int tile = 0; tile < ntiles; ++tile) nn += part_nrm[static_cast<size_t>(tile) * ldm + t];
+        const double b = sqrt(nn);
+        beta0[t] = b;
+        inv0[t] = b > 0.0 ? 1.0 / b : 0.0;
+        if (!isfinite(b)) bad = true;
+    }
+    if (bad) atomicOr(status, 2);
+}
+
+// Ensemble value of this time point, values_out[o] = sum over trajectories
+// t < M of prev[o][t], summed in k_yield_update's order (thread-strided, then
+// warps, then the warp totals).  One CTA of 1024 threads.
+__global__ void __launch_bounds__(1024)
+k_yield_values(const double *__restrict__ prev, int nobs, int ldm, int M, double *__restrict__ values_out)
+{
+    __shared__ double red[8][32];
+    double ens[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = threadIdx.x; t < ldm; t += blockDim.x)
+        for (int o = 0; o < nobs; ++o)
+            if (t < M) ens[o] += prev[static_cast<size_t>(o) * ldm + t];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 0; o < nobs; ++o) {
+        double v = warp_sum(ens[o]);
+        if (lane == 0) red[o][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nobs) {
+        double s = 0.0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        values_out[threadIdx.x] = s;
+    }
+}
+
 template <typename Dst, typename Src>
 __global__ void k_convert(Dst *__restrict__ out, const Src *__restrict__ in, size_t n)
 {
