@@ -1059,7 +1059,12 @@ int build_quartet(msgpu_ctx *c)
         }
         std::vector<size_t> ord(blocks.size());
         for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
-        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return blocks[x].first < blocks[y].first; });
+        // by neighbour base, the quartet's own block last (the SpMM reuses its
+        // gathered rows for the alpha partial)
+        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+            const bool ox = blocks[x].first == b, oy = blocks[y].first == b;
+            return ox != oy ? oy : blocks[x].first < blocks[y].first;
+        });
         for (size_t oi : ord) {
             const auto &blk = blocks[oi];
             const auto &B = blk.second;  // 16 complex, row-major in the pair index

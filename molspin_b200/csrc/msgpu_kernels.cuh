@@ -487,18 +487,24 @@ k_lanczos_apply_np(QuartetC H, const float2 *__restrict__ wj, const double *__re
 #pragma unroll
             for (int a = 0; a < 4; ++a) o[k][a][0] = o[k][a][1] = make_float2(0.f, 0.f);
         const int kb = __ldg(H.rowptr + q), ke = __ldg(H.rowptr + q + 1);
+        // The host stores each quartet's own (diagonal) block last, so the
+        // gathered rows of the final block are v_j at this quartet's rows and
+        // serve the alpha partial below without a second read.
+        float4 x[NP][4];
+        int last = -1;
         for (int kk = kb; kk < ke; ++kk) {
             const int2 cur = __ldg(H.blk + kk);
-            float4 x[NP][4];
+            last = cur.x >> 3;
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const float2 *row = wj + static_cast<size_t>((cur.x >> 3) + off[b]) * ldm + tb;
+                const float2 *row = wj + static_cast<size_t>(last + off[b]) * ldm + tb;
 #pragma unroll
                 for (int k = 0; k < NP; ++k) x[k][b] = *reinterpret_cast<const float4 *>(row + 64 * k);
             }
             quartet_block_np<NP>(o, cur.x & 7, H.val + cur.y, x);
         }
         const int base = __ldg(H.base + q);
+        const bool own = last == base;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const size_t e = static_cast<size_t>(base + off[a]) * ldm + tb;
@@ -507,7 +513,7 @@ k_lanczos_apply_np(QuartetC H, const float2 *__restrict__ wj, const double *__re
                 const float2 ure = make_float2(o[k][a][0].x * sc[k][0], o[k][a][0].y * sc[k][1]);
                 const float2 uim = make_float2(o[k][a][1].x * sc[k][0], o[k][a][1].y * sc[k][1]);
                 *reinterpret_cast<float4 *>(U + e + 64 * k) = make_float4(ure.x, ure.y, uim.x, uim.y);
-                const float4 v = *reinterpret_cast<const float4 *>(wj + e + 64 * k);
+                const float4 v = own ? x[k][a] : *reinterpret_cast<const float4 *>(wj + e + 64 * k);
                 acc[k][0] += (static_cast<double>(v.x) * ure.x + static_cast<double>(v.z) * uim.x) * sc[k][0];
                 acc[k][1] += (static_cast<double>(v.y) * ure.y + static_cast<double>(v.w) * uim.y) * sc[k][1];
             }
