@@ -96,9 +96,12 @@ def to_csr(A: np.ndarray, tol: float = 0.0):
     return (m.indptr.astype(np.int32), m.indices.astype(np.int32), m.data.astype(np.complex128))
 
 
+# |S> = (|ud> - |du>)/sqrt(2) in the pair basis uu, ud, du, dd (digit 0 = m=+1/2)
+SINGLET = np.array([0.0, 1.0, -1.0, 0.0], dtype=np.complex128) / np.sqrt(2.0)
+
+
 def singlet_density(system) -> np.ndarray:
     """rho0 = |S><S| x I_Z / Z (the trace-sampled initial state's expectation)."""
-    from molspin_b200.systems import SINGLET
     P = pair_operator(np.outer(SINGLET, SINGLET.conj()), system)
     return P / np.trace(P).real
 
