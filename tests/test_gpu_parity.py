@@ -24,7 +24,7 @@ FORMS = ["streamed", "resident"]
 
 
 def _gpu(system, factors, times, krylov, precision="c128", noise=None, K_csr=None, kappa=None,
-         obs=None, chunks=None, form="auto"):
+         obs=None, chunks=None, form="auto", propagator="krylov"):
     with hs.HSPropagatorB200(0) as p:
         p.set_form(form)
         p.set_hamiltonian(*system.hamiltonian_csr())
@@ -39,7 +39,7 @@ def _gpu(system, factors, times, krylov, precision="c128", noise=None, K_csr=Non
             p.set_noise(*noise)
         p.set_factors(factors)
         if chunks is None:
-            p.propagate(times, krylov, precision)
+            p.propagate(times, krylov, precision, propagator=propagator)
             values = p.values()
         else:
             values = []
@@ -142,15 +142,22 @@ def test_exact_trace_against_density_oracle(form):
     assert _rel(values, dv) < 1e-10
 
 
-def test_stochastic_st_against_lindblad_and_survival():
-    # GeneralStatic fixture of the reference on the GPU (8192 samples, m=8)
+@pytest.mark.parametrize("propagator", ["krylov", "taylor"])
+def test_stochastic_st_against_lindblad_and_survival(propagator):
+    # The reference's Tests/StochasticRelaxation/st_dephasing.msd on the GPU: 8192 samples with
+    # seed 431, dt 0.025 over 2 ns, its stochastic task's propagationmethod=autoexpm with
+    # precision=double (the Taylor propagator) and the Krylov step (m=8); the bounds of its
+    # check_output.py: populations within 6/(2 sqrt(8192)) of the exact density dynamics and
+    # total survival within 2e-6 of exp(-0.2 t).
     system = h.st_fixture()
     times = S.time_grid(2.0, 0.025)
     M = 8192
     F = system.trace_samples(M, 431.0)
     pops = [(S.pair_projector(S.PAIR_STATES[n]), 1.0) for n in ("S", "T0", "Tp", "Tm")]
     bits = hs.reference_flip_bits(431.0, 0.7, times, M)
-    _, _, values, _ = _gpu(system, F, times, 8, noise=(0.7, L.NOISE_REPLAY, 0, bits, len(times) - 1, M), obs=pops)
+    _, _, values, _ = _gpu(system, F, times, 8, noise=(0.7, L.NOISE_REPLAY, 0, bits, len(times) - 1, M), obs=pops,
+                           propagator=propagator)
+    assert values.shape == (81, 4)
     assert np.max(np.abs(values.sum(axis=1) - np.exp(-0.2 * times))) < 2e-6
     H = den.dense_hamiltonian(system)
     K = 0.1 * np.eye(system.dim)
