@@ -274,9 +274,9 @@ long long msgpu_batch_launch_count(const msgpu_batch *batch);
 long long msgpu_launch_count(const msgpu_ctx *ctx);
 
 /* No counterpart in the reference.  For callers that cannot allocate device
- * memory (for example code running inside a CUDA-graph capture or under a
- * memory pool that forbids cudaMalloc, or a host framework that owns all
- * allocations): one Krylov step psi_out = exp(dt (-iH - kappa I)) psi_in for
+ * memory (for example an embedding host framework whose memory pool owns
+ * all device memory, or code on a latency-critical path that must not take
+ * the implicit device synchronisation of cudaMalloc / cudaFree): one Krylov step psi_out = exp(dt (-iH - kappa I)) psi_in for
  * every trajectory column, computed with the complex128 Arnoldi kernels of
  * msgpu_run, using only the caller's buffers and a fixed static scratch area
  * of MSGPU_NOALLOC_SCRATCH_BYTES compiled into this library (held on every

@@ -2060,9 +2060,10 @@ int msgpu_profile_read(msgpu_ctx *c, int cls, double *total_ms, long long *launc
 // ============================================================================
 // Allocation-free Krylov step (msgpu_krylov_step_noalloc).
 //
-// Some callers cannot call cudaMalloc: code that runs while a stream is being
-// captured into a CUDA graph, hosts whose memory pool owns every device
-// allocation, or embedders that must bound device memory at load time.  For
+// Some callers cannot call cudaMalloc: hosts whose memory pool owns every
+// device allocation, code that must not take the implicit device
+// synchronisation of cudaMalloc / cudaFree, or embedders that must bound
+// device memory at load time.  For
 // them this entry point runs one complex128 Arnoldi step with all of its
 // temporaries in one static device array.  The array lives in this library
 // image, so every GPU that loads the library holds MSGPU_NOALLOC_SCRATCH_BYTES

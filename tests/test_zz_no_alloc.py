@@ -1,7 +1,8 @@
 """The allocation-free Krylov step (msgpu_krylov_step_noalloc).
 
-Callers that cannot allocate device memory -- code recording a CUDA graph,
-hosts whose memory pool owns every allocation -- get one Krylov step that
+Callers that cannot allocate device memory -- hosts whose memory pool owns
+every allocation, code that must not take the implicit device
+synchronisation of cudaMalloc / cudaFree -- get one Krylov step that
 uses only their buffers and the library's static scratch area.  Here it is
 called through the C ABI with caller-owned device buffers and compared with
 the regular entry point (msgpu_run of one step followed by
