@@ -39,9 +39,12 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk", type=int, default=50, help="time steps per bench step")
     ap.add_argument("--traj", type=int, default=1024)
-    ap.add_argument("--plain-steps", type=int, default=4, help="time steps of the complex128 comparison run")
+    ap.add_argument("--plain-steps", type=int, default=50,
+                    help="time steps of the complex128 comparison run (one bench step)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-segments", action="store_true",
+                    help="precision line only (no dense, batching and serving segments)")
     ap.add_argument("--workload", default="precision", choices=["precision", "plain", "dense", "batching", "serving"],
                     help="precision (default line): D=16384 complex64; plain: D=64 complex128; dense: D=1024 "
                          "tensor-core propagator; batching: 64 uneven systems; serving: a request stream")
@@ -133,23 +136,30 @@ CPU_SAMPLE_STEPS = 128  # precision workload: 2 trajectories per core x 128 step
 TRAFFIC_SPMM = {(16384, 1024): 243.9e6, (16384, 512): 117.5e6}
 
 
-def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
-    """The CPU restatement (complex128 Arnoldi/MGS, per-column Krylov) on a bounded sample."""
+def _oracle_inputs(w, traj: int, steps: int):
+    """Inputs of a CPU sample built by the oracle alone (trace samples, sparse Kronecker H,
+    pair observables, time grid), so that the CPU legs never load the product library."""
     from oracle import density as den
     from oracle import pyoracle as orc
     from molspin_b200 import systems as S
-    F = w.system.trace_samples(sample_traj, w.seed)
-    times = S.time_grid(sample_steps * w.dt, w.dt)
-    obs = [(den.to_csr(den.pair_operator(op, w.system)), rate) for _, op, rate in w.system.observables()]
-    Hc = w.system.hamiltonian_csr()
+    F = orc.trace_samples(float(w.seed), S.SINGLET, w.system.dim // 4, traj)
+    times = orc.time_grid(steps * w.dt, w.dt)
+    obs = [(den.pair_operator_csr(op, w.system), rate) for _, op, rate in w.system.observables()]
+    return F, times, obs, den.sparse_hamiltonian(w.system)
+
+
+def cpu_reference(w, sample_traj: int, sample_steps: int, threads: int) -> dict:
+    """The CPU restatement (complex128 Arnoldi/MGS, per-column Krylov) on a bounded sample."""
+    from oracle import pyoracle as orc
+    F, times, obs, Hc = _oracle_inputs(w, sample_traj, sample_steps)
     orc.hs_stochastic(Hc, F[:, :threads], times[:2], obs, kappa=w.system.kappa(), krylov=w.krylov,
                       nthreads=threads)  # warm-up
     t0 = time.perf_counter()
     orc.hs_stochastic(Hc, F, times, obs, kappa=w.system.kappa(), krylov=w.krylov, nthreads=threads)
     el = time.perf_counter() - t0
     return {"value": sample_traj * sample_steps / el, "unit": "traj-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{sample_traj} trajectories x {sample_steps} steps of the D=16384 m=20 workload "
-                      f"(complex128 Arnoldi, {el:.1f} s)"}
+            "sample": f"{sample_traj} trajectories x {sample_steps} steps of the D={w.system.dim} m={w.krylov} "
+                      f"workload (complex128 Arnoldi, {el:.1f} s)"}
 
 
 def run_reference(args):
@@ -259,8 +269,11 @@ def run_ours(args):
     achieved = alg_bytes / apply_avg_s / 1e9 if apply_n else None
     # the whole time step against HBM: m SpMMs, m-1 updates (4 vectors each) and
     # the combine ((m + 2) vectors); expm, reductions and yields are negligible
+    # the minimal fused Krylov traffic per time step, (4m+1) D c per trajectory (c = 8 B), and the
+    # traffic of the kernels as they are split here (m SpMMs, m-1 four-vector updates, the combine)
     m_k = w.krylov
-    step_bytes = m_k * groups * alg_bytes + (m_k - 1) * 4 * D * M * 8 + (m_k + 2) * D * M * 8
+    step_bytes = (4 * m_k + 1) * D * 8 * M
+    step_bytes_split = m_k * groups * alg_bytes + (m_k - 1) * 4 * D * M * 8 + (m_k + 2) * D * M * 8
     step_s = el_max / 1e3 / (K * chunk)
 
     # plain complex128 path (reference-faithful Arnoldi) on a short segment,
@@ -315,6 +328,8 @@ def run_ours(args):
         cpu = cpu_reference(w, 2 * threads, CPU_SAMPLE_STEPS, threads)
 
     p.close()
+    segments = {} if args.no_segments else run_segments(args)
+    line = None
     if rank == 0:
         line = {
             "metric": "SSE traj-steps/s (stochastic HSGeneral, Krylov m=20, D=16384)",
@@ -332,9 +347,13 @@ def run_ours(args):
                          "timing": "CUDA events around every launch of every 32nd time step (sampled)",
                          "share_of_step": apply_avg_s * 1e3 * w.krylov * groups * chunk * K / el_ms if el_ms else None,
                          "trajectories_per_launch": width},
-            "step_roofline": {"bound": "hbm", "alg_bytes_per_time_step": step_bytes, "time_step_ms": step_s * 1e3,
+            "step_roofline": {"bound": "hbm", "alg_bytes_per_time_step": step_bytes,
+                              "alg_bytes": "(4m+1) D c per trajectory: the minimal fused Krylov traffic",
+                              "time_step_ms": step_s * 1e3,
                               "achieved": step_bytes / step_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                              "frac": step_bytes / step_s / 1e9 / hbm_peak, "peak_kind": peak_kind},
+                              "frac": step_bytes / step_s / 1e9 / hbm_peak, "peak_kind": peak_kind,
+                              "split_kernel_bytes_per_time_step": step_bytes_split,
+                              "split_kernel_frac": step_bytes_split / step_s / 1e9 / hbm_peak},
             "kernel_avg_ms": {"apply": apply_ms / max(1, apply_n), "update": orth_ms / max(1, orth_n),
                               "combine": comb_ms / max(1, comb_n),
                               **({"lanczos_cluster_resident": fused_ms / fused_n} if fused_n else {})},
@@ -346,9 +365,31 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "cpu_baseline": cpu,
+            "segments": segments,
         }
-        print(json.dumps(line), flush=True)
-    ranks.finish(world)
+    return rank, line
+
+
+def run_segments(args) -> dict:
+    """Short driver-clocked runs of the other configurations after the contract line (each with
+    its own clocks, launch count and roofline where one applies): the dense tensor-core form
+    (config 4 shape, 1000 timed steps), the batching form (the 64-system batch, 200 timed steps)
+    and a serving stream below saturation (12 requests of the serving mix at 0.25 requests/s)."""
+    import copy
+    out = {}
+    for name, fn, kw in (("dense", run_dense, dict(chunk=500, steps=2, warmup=3)),
+                         ("batching", run_batching, dict(chunk=100, steps=2, warmup=3)),
+                         ("serving", run_serving, dict(requests=12, rate=0.25))):
+        a = copy.copy(args)
+        a.no_cpu = True
+        a.traj = 1024  # the runners' own defaults
+        for k, v in kw.items():
+            setattr(a, k, v)
+        _, line = fn(a)
+        if line is not None:
+            line.pop("cpu_baseline", None)
+            out[name] = line
+    return out
 
 
 def _peaks() -> dict:
@@ -415,16 +456,11 @@ def _e2e(p, world, F, times, krylov, precision, propagator, E):
 
 def _cpu_port(w, traj: int, steps: int, method: int = 0) -> dict:
     """The oracle (CPU restatement of the reference algorithm) on all host cores."""
-    from oracle import density as den
     from oracle import pyoracle as orc
-    from molspin_b200 import systems as S
     threads = os.cpu_count() or 1
-    F = w.system.trace_samples(traj, w.seed)
-    times = S.time_grid(steps * w.dt, w.dt)
-    obs = [(den.to_csr(den.pair_operator(op, w.system)), rate) for _, op, rate in w.system.observables()]
+    F, times, obs, Hc = _oracle_inputs(w, traj, steps)
     t0 = time.perf_counter()
-    orc.hs_stochastic(w.system.hamiltonian_csr(), F, times, obs, kappa=w.system.kappa(), krylov=w.krylov,
-                      method=method, nthreads=threads)
+    orc.hs_stochastic(Hc, F, times, obs, kappa=w.system.kappa(), krylov=w.krylov, method=method, nthreads=threads)
     el = time.perf_counter() - t0
     return {"value": traj * steps / el, "unit": "traj-steps/s", "cores": threads, "kind": "port",
             "sample": f"{traj} trajectories x {steps} steps of {w.name} ({el:.1f} s)"}
@@ -459,7 +495,7 @@ def run_plain(args):
     e2e = None if args.no_e2e else _e2e(p, world, F, times, w.krylov, "c128", "krylov", max(1, min(args.steps, 3)))
     p.close()
     cpu = _cpu_port(w, w.M, w.steps) if rank == 0 and world == 1 and not args.no_cpu else None  # the whole workload
-    _emit(rank, {
+    return rank, ({
         "metric": "SSE traj-steps/s (plain complex128, D=64, m=16)", "value": world * w.M * chunk * args.steps / (el / 1e3),
         "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -531,7 +567,7 @@ def run_dense(args):
     p.close()
     # the reference has no dense propagator: its CPU path is the Krylov step
     cpu = _cpu_port(w, 8 * (os.cpu_count() or 1), 600) if rank == 0 and world == 1 and not args.no_cpu else None
-    _emit(rank, {
+    return rank, ({
         "metric": "SSE traj-steps/s (dense tensor-core propagator, D=1024)",
         "value": world * M * chunk * args.steps / (el / 1e3), "unit": "traj-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
@@ -586,7 +622,14 @@ def run_batching(args):
     st = bt.stats()
     Mtot = sum(w.M for w in ws)
     bt.close()
-    _emit(rank, {
+    # whole-batch HBM roofline with the minimal fused Krylov traffic (4m+1) D c per traj-step
+    # (complex64, c = 8 B); the persistent kernel keeps small systems on chip, so this is the
+    # bound the streamed large systems face
+    bytes_per_step = sum((4 * 16 + 1) * w.system.dim * 8 * w.M for w in ws)
+    peaks = _peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = bytes_per_step * chunk * args.steps / (el / 1e3) / 1e9 if el else None
+    return rank, ({
         "metric": "SSE traj-steps/s (batching form, 64 uneven systems)",
         "value": world * Mtot * chunk * args.steps / (el / 1e3), "unit": "traj-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
@@ -594,7 +637,10 @@ def run_batching(args):
         "config": {"workload": "64 radical pairs, 4-10 nuclei (0-2 spin-1), dims 64-9216, M 64-1024, dt=1 ns",
                    "trajectories_per_gpu": Mtot, "time_steps_per_bench_step": chunk, "team_threshold": st["team_threshold"],
                    "ctas_per_sm": st["ctas_per_sm"], "tune_s": tune_s},
-        "roofline": None, "clocks": clk, "e2e": None, "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "whole batch ((4m+1) D c bytes per traj-step)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                     "traffic": None, "peak_kind": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "clocks": clk, "e2e": None, "gpu_launches": launches,
         "launch_note": "per bench step: one graph replay of the persistent k_batch launch (systems below D=2048) "
                        "plus the streamed path's kernels for the larger systems", "cpu_baseline": None})
 
@@ -620,7 +666,14 @@ def run_serving(args):
     el = _max_over_ranks(time.perf_counter() - t0, world)
     clk = clocks.stop()
     s = SV.summarize(res)
-    _emit(rank, {
+    # HBM roofline of the whole stream with the minimal fused Krylov traffic (4m+1) D c per
+    # traj-step (complex64, c = 8 B)
+    total_bytes = sum((4 * r.workload.krylov + 1) * r.workload.system.dim * 8 * r.workload.M * r.workload.steps
+                      for r in reqs) * world
+    peaks = _peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = total_bytes / el / 1e9
+    return rank, ({
         "metric": "SSE traj-steps/s (serving form, continuous batching)", "value": world * s["traj_steps"] / el,
         "unit": "traj-steps/s", "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": el * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP64 reductions/expm/sums)",
@@ -629,7 +682,11 @@ def run_serving(args):
                    "slots": 8, "hbm_budget_gib": 120},
         "latency_s": {"p50": s["p50_latency_s"], "p99": s["p99_latency_s"], "mean": s["mean_latency_s"]},
         "completed": s["completed"], "failed": s["failed"], "max_concurrency": eng.max_concurrency,
-        "peak_reserved_gib": eng.peak_reserved / 2 ** 30, "roofline": None, "clocks": clk, "e2e": None,
+        "peak_reserved_gib": eng.peak_reserved / 2 ** 30,
+        "roofline": {"bound": "hbm", "kernel": "whole stream ((4m+1) D c bytes per traj-step)", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "peak_kind": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "clocks": clk, "e2e": None,
         "gpu_launches": None, "cpu_baseline": None})
 
 
@@ -637,16 +694,11 @@ def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "plain":
-        run_plain(args)
-    elif args.workload == "dense":
-        run_dense(args)
-    elif args.workload == "batching":
-        run_batching(args)
-    elif args.workload == "serving":
-        run_serving(args)
     else:
-        run_ours(args)
+        runner = {"plain": run_plain, "dense": run_dense, "batching": run_batching, "serving": run_serving,
+                  "precision": run_ours}[args.workload]
+        rank, line = runner(args)
+        _emit(rank, line)
     from molspin_b200 import ranks
     ranks.finish(int(os.environ.get("WORLD_SIZE", "1")))
 

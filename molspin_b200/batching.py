@@ -4,9 +4,14 @@ The reference propagates the systems of a powder average or parameter sweep
 one after another: the orientation loop of ``TaskHSGeneral::RunLocal``
 (RunSection/General/HS/TaskHSGeneral.cpp:347) and the RunSection step loop
 (main.cpp:651-678) each re-run the whole HSGeneral time loop.  Here every
-(system, trajectory) pair of a batch advances inside ONE persistent kernel
-launch (msgpu_batch_* in include/msgpu.h), replayed from a CUDA graph, with
-the team threshold and grid size chosen by an autotuner on the batch.
+(system, trajectory) pair of a system below the streamed-route dimension
+(2048) advances inside ONE persistent kernel launch (msgpu_batch_* in
+include/msgpu.h), replayed from a CUDA graph, with the team threshold and
+grid size chosen by an autotuner on the batch.  Systems at or above that
+dimension run the streamed precision form (quartet SpMM over the whole
+trajectory block) on their own contexts and streams, concurrently with the
+persistent launch: a persistent team propagates one trajectory at a time
+and re-reads H per trajectory, which loses to the lockstep SpMM there.
 """
 from __future__ import annotations
 

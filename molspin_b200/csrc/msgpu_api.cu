@@ -2080,8 +2080,11 @@ constexpr int kNoallocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void *g_noalloc_ptr[kNoallocMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up on
-// the first call per device).
+// Device address of the scratch array on the current device.  It is looked
+// up on the first call per device; later calls check that the cached address
+// still belongs to a live device allocation of that device (a
+// cudaDeviceReset unloads the library image and the array moves when the
+// context is recreated) and look it up again when it does not.
 cudaError_t noalloc_scratch(void **out)
 {
     int dev = 0;
@@ -2089,6 +2092,14 @@ cudaError_t noalloc_scratch(void **out)
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[dev]) {
+        cudaPointerAttributes attr;
+        const cudaError_t ae = cudaPointerGetAttributes(&attr, g_noalloc_ptr[dev]);
+        if (ae != cudaSuccess || attr.type != cudaMemoryTypeDevice || attr.device != dev) {
+            if (ae != cudaSuccess) (void)cudaGetLastError();  // this probe's own error only
+            g_noalloc_ptr[dev] = nullptr;
+        }
+    }
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -2122,6 +2133,14 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
         return MSGPU_ERR_INVALID;
     if (krylov_dim < 1 || krylov_dim > kMaxKrylov || !std::isfinite(dt) || !(dt > 0.0) || !std::isfinite(kappa))
         return MSGPU_ERR_INVALID;
+    // The state alone takes 16 bytes per (row, trajectory) and dim >= 4, so a
+    // trajectory count above this bound cannot fit; refusing it here keeps the
+    // index arithmetic below free of overflow.
+    if (static_cast<size_t>(ntraj) > MSGPU_NOALLOC_SCRATCH_BYTES / 64) return MSGPU_ERR_SCRATCH;
+    if (static_cast<size_t>(dim) > MSGPU_NOALLOC_SCRATCH_BYTES / 16) return MSGPU_ERR_SCRATCH;
+    // An error the caller left pending belongs to the caller: report it
+    // without clearing it, before queuing anything.
+    if (cudaPeekAtLastError() != cudaSuccess) return MSGPU_ERR_CUDA;
     const int D = dim, m = std::min(krylov_dim, dim);
     const int ldm = (ntraj + 63) / 64 * 64;
     const size_t n = static_cast<size_t>(D) * ldm;

@@ -29,8 +29,6 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _lib as L
-
 COMMON_PREFACTOR = 8.79410005e1  # rad ns^-1 T^-1
 G_ELECTRON = 2.0023
 
@@ -86,6 +84,7 @@ class SpinSystem:
     # ------------------------------------------------------------ host builder
     def hamiltonian_csr(self):
         """H in rad/ns as CSR (rowptr int32, col int32, val complex128)."""
+        from . import _lib as L
         mult = np.asarray(self.mult, dtype=np.int32)
         lin_spin = np.asarray([k for k, _ in self.linear], dtype=np.int32)
         lin_w = np.ascontiguousarray(np.array([w for _, w in self.linear], dtype=np.float64).reshape(-1))
@@ -110,6 +109,7 @@ class SpinSystem:
         (reference fast path; requires the electrons to be the leading spins)."""
         if tuple(self.electrons) != (0, 1):
             raise ValueError("the tensor fast path needs the radical pair as the two leading spins")
+        from . import _lib as L
         F, Z = 4, self.dim // 4
         fixed = np.ascontiguousarray(PAIR_STATES[state])
         out = np.zeros((M, self.dim), dtype=np.complex128)  # row t = column t of the D x M matrix
@@ -300,6 +300,7 @@ def sphere_grid(n: int) -> np.ndarray:
 
 def time_grid(total: float, dt: float) -> np.ndarray:
     """Exact-endpoint free-evolution grid (TaskHSGeneral.cpp:59-96)."""
+    from . import _lib as L
     n = L.lib.msgpu_host_time_grid(float(total), float(dt), None, 0)
     if n < 0:
         raise ValueError("invalid time grid")

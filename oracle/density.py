@@ -56,6 +56,61 @@ def dense_hamiltonian(system) -> np.ndarray:
     return H
 
 
+def _sparse_embed(ops: dict, mult: list[int]):
+    out = sp.identity(1, dtype=np.complex128, format="csr")
+    for k, d in enumerate(mult):
+        out = sp.kron(out, sp.csr_matrix(ops[k]) if k in ops else sp.identity(d, dtype=np.complex128), format="csr")
+    return out
+
+
+def sparse_hamiltonian(system):
+    """H as CSR (rowptr, col, val) for dimensions where the dense assembly does not fit: the same
+    Kronecker terms as dense_hamiltonian, with scipy.sparse products."""
+    mult = system.mult
+    S = [spin_matrices(d) for d in mult]
+    D = int(np.prod(mult))
+    H = sp.csr_matrix((D, D), dtype=np.complex128)
+    for k, w in system.linear:
+        for a in range(3):
+            if w[a] != 0.0:
+                H = H + w[a] * _sparse_embed({k: S[k][a]}, mult)
+    for i, j, Cm in system.bilinear:
+        for a in range(3):
+            for b in range(3):
+                if Cm[a][b] != 0.0:
+                    H = H + Cm[a][b] * _sparse_embed({i: S[i][a], j: S[j][b]} if i != j else
+                                                     {i: S[i][a] @ S[j][b]}, mult)
+    H = H.tocsr()
+    H.eliminate_zeros()
+    H.sort_indices()
+    return (H.indptr.astype(np.int32), H.indices.astype(np.int32), H.data.astype(np.complex128))
+
+
+def pair_operator_csr(op4: np.ndarray, system):
+    """pair_operator as CSR, without forming the dense D x D matrix."""
+    e1, e2 = system.electrons
+    D = system.dim
+    strides = system.strides()
+    idx = np.arange(D)
+    d1 = (idx // strides[e1]) % 2
+    d2 = (idx // strides[e2]) % 2
+    base = idx - d1 * strides[e1] - d2 * strides[e2]
+    rows, cols, vals = [], [], []
+    for a in range(4):
+        for b in range(4):
+            v = op4[a, b]
+            if v == 0:
+                continue
+            r = np.nonzero((2 * d1 + d2) == a)[0]
+            rows.append(r)
+            cols.append(base[r] + (b >> 1) * strides[e1] + (b & 1) * strides[e2])
+            vals.append(np.full(len(r), v, dtype=np.complex128))
+    m = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(D, D))
+    m.sum_duplicates()
+    m.sort_indices()
+    return (m.indptr.astype(np.int32), m.indices.astype(np.int32), m.data.astype(np.complex128))
+
+
 def pair_operator(op4: np.ndarray, system) -> np.ndarray:
     """Embed a 4x4 operator on the radical pair (basis |e1 e2>, digit 0 = up)."""
     mult = system.mult
@@ -119,6 +174,46 @@ def lindblad_exact(H: np.ndarray, K: np.ndarray, rho0: np.ndarray, t: float, U: 
         Lg = Lg + lam * (np.kron(U, U.conj()) - np.eye(D * D))
     v = sla.expm(t * Lg) @ rho0.reshape(-1)
     return v.reshape(D, D)
+
+
+def st_dephasing_rk4(H: np.ndarray, K: np.ndarray, rho0: np.ndarray, times: np.ndarray, observables,
+                     U: np.ndarray, st_rate: float) -> np.ndarray:
+    """The reference's deterministic ("direct") HSGeneral arm with an ST-dephasing Operator:
+    one classical RK4 step of the density matrix per grid interval
+    (HSPropagator::StepDensity, RunSection/General/HS/HSPropagator.cpp:152-189) on
+        d rho/dt = -i[H, rho] - {K, rho} - k (P_T rho P_S + P_S rho P_T),
+    the dephasing term of SpinSpace::ApplyRelaxationHilbert
+    (SpinAPI/SpinSpace/SpinSpace_relaxation.cpp:695-716), with P_S = (1 + U)/2,
+    P_T = 1 - P_S.  Observables are evaluated before every step
+    (TaskHSGeneral.cpp:471-560).  Returns values[(ntimes) x nobs] of rate * Tr(O rho)."""
+    D = H.shape[0]
+    PS = 0.5 * (np.eye(D) + U)
+    PT = np.eye(D) - PS
+
+    def rhs(r):
+        return -1j * (H @ r - r @ H) - (K @ r + r @ K) - st_rate * (PT @ r @ PS + PS @ r @ PT)
+
+    rho = rho0.astype(np.complex128).copy()
+    values = np.zeros((len(times), len(observables)))
+    for s in range(len(times)):
+        values[s] = [rate * np.trace(O @ rho).real for O, rate in observables]
+        if s + 1 == len(times):
+            break
+        dt = times[s + 1] - times[s]
+        k1 = rhs(rho)
+        k2 = rhs(rho + 0.5 * dt * k1)
+        k3 = rhs(rho + 0.5 * dt * k2)
+        k4 = rhs(rho + dt * k3)
+        rho = rho + (dt / 6.0) * (k1 + 2.0 * k2 + 2.0 * k3 + k4)
+    return values
+
+
+def data_file_difference(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a - b| over the values as the reference's data file prints them (12 significant
+    digits, TaskHSGeneral.cpp:642-646), as Tests/StochasticRelaxation/check_output.py reads them."""
+    def printed(x):
+        return np.array([[float(f"{v:.12g}") for v in row] for row in np.atleast_2d(x)])
+    return float(np.max(np.abs(printed(a) - printed(b))))
 
 
 def propagate_density(H: np.ndarray, K: np.ndarray, rho0: np.ndarray, times: np.ndarray, observables,

@@ -62,3 +62,23 @@ def survival_bound():
 
 def six_sigma(M: int) -> float:
     return 6.0 / (2.0 * math.sqrt(M))
+
+
+# The reference's recorded result for its input-file example
+# Tests/StochasticRelaxation/st_dephasing.msd (8192 samples, seed 431, dt 0.025 ns over 2 ns):
+# max |stochastic - direct| population difference over the 81 x 4 data-file values
+# (RunSection/General/HS/STOCHASTIC_RELAXATION.md:250-251), printed to 8 significant digits.
+ST_DEPHASING_POPULATION_ERROR = 0.0012766377
+# Tolerance: half a unit of the recorded figure's last digit plus the propagators'
+# own differences (every one of the reference's propagators records 0.00127664, :236).
+ST_DEPHASING_PIN_TOL = 1e-10
+
+
+def st_dephasing_direct(system, times):
+    """The example's "direct" task (sampling=direct; propagationmethod=rk4) on the same grid:
+    density-matrix RK4 with the ST dephasing Operator; S, T0, T+, T- populations."""
+    H = den.dense_hamiltonian(system)
+    K = 0.5 * system.sinks["S"] * np.eye(system.dim)
+    ops = [(den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), system), 1.0) for n in ("S", "T0", "Tp", "Tm")]
+    return den.st_dephasing_rk4(H, K, den.singlet_density(system), times, ops, den.st_unitary(system),
+                                system.st_rate)

@@ -146,9 +146,9 @@ def test_exact_trace_against_density_oracle(form):
 def test_stochastic_st_against_lindblad_and_survival(propagator):
     # The reference's Tests/StochasticRelaxation/st_dephasing.msd on the GPU: 8192 samples with
     # seed 431, dt 0.025 over 2 ns, its stochastic task's propagationmethod=autoexpm with
-    # precision=double (the Taylor propagator) and the Krylov step (m=8); the bounds of its
-    # check_output.py: populations within 6/(2 sqrt(8192)) of the exact density dynamics and
-    # total survival within 2e-6 of exp(-0.2 t).
+    # precision=double (the Taylor propagator) and the Krylov step (m=8), with the reference's
+    # own flip stream replayed.  The population difference from the direct task must equal the
+    # value the reference recorded for this example, and survival must be at its 1e-12 level.
     system = h.st_fixture()
     times = S.time_grid(2.0, 0.025)
     M = 8192
@@ -158,14 +158,13 @@ def test_stochastic_st_against_lindblad_and_survival(propagator):
     _, _, values, _ = _gpu(system, F, times, 8, noise=(0.7, L.NOISE_REPLAY, 0, bits, len(times) - 1, M), obs=pops,
                            propagator=propagator)
     assert values.shape == (81, 4)
-    assert np.max(np.abs(values.sum(axis=1) - np.exp(-0.2 * times))) < 2e-6
-    H = den.dense_hamiltonian(system)
-    K = 0.1 * np.eye(system.dim)
-    rho0 = den.singlet_density(system)
-    U = den.st_unitary(system)
-    direct = np.array([[np.trace(den.pair_operator(op, system) @ den.lindblad_exact(H, K, rho0, t, U, 0.7)).real
-                        for op, _ in pops] for t in times])
-    assert np.max(np.abs(values - direct)) < h.six_sigma(M)
+    surv = np.max(np.abs(values.sum(axis=1) - np.exp(-0.2 * times)))
+    assert surv < 1e-11, surv  # the reference recorded 8.129053e-13 (check_output.py bound: 2e-6)
+    # the reference's recorded population error of this example against its direct task
+    # (density-matrix RK4), STOCHASTIC_RELAXATION.md:250-251: 0.0012766377
+    err = den.data_file_difference(values, h.st_dephasing_direct(system, times))
+    assert abs(err - h.ST_DEPHASING_POPULATION_ERROR) < h.ST_DEPHASING_PIN_TOL, err
+    assert err < h.six_sigma(M)
 
 
 @pytest.mark.parametrize("form", FORMS)

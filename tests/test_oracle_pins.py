@@ -135,10 +135,15 @@ def test_st_reproducibility_and_noop():
     np.testing.assert_array_equal(a["values"], c["values"])
 
 
-@pytest.mark.slow
-def test_general_static_survival_and_density():
-    # GeneralStatic (:197-217): E1,E2,N; 4 sinks k=0.2; Z = 0.8 Sz(E1); ST 0.7;
-    # totaltime 2, timestep 0.025, seed 431, 8192 samples, krylov m=8.
+def test_st_dephasing_example_reproduces_recorded_error():
+    # The reference's input-file example Tests/StochasticRelaxation/st_dephasing.msd: E1, E2, N;
+    # four sinks k=0.2; Z = 0.8 Sz(E1); ST dephasing 0.7; totaltime 2, timestep 0.025, seed 431,
+    # 8192 samples.  Its check_output.py compares the stochastic task's data file with the direct
+    # task's (density-matrix RK4) and the reference recorded the maximum population difference
+    # 0.0012766377 and survival error 8.129053e-13 (STOCHASTIC_RELAXATION.md:250-251).  The value
+    # is set by the seeded trace-sample and flip streams and the loop order, so matching it to
+    # 1e-10 ties all three to the reference's own numbers.  Every propagator of the oracle must
+    # reproduce it (the reference records the same for each of its propagators, :236).
     system = h.st_fixture()
     times = orc.time_grid(2.0, 0.025)
     M = 8192
@@ -146,21 +151,35 @@ def test_general_static_survival_and_density():
     Hc = h.dense_csr(system)
     obs = h.state_population_observables(system)
     Uc = orc.st_unitary(system.mult, 0, 1)
-    out = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=8, U_csr=Uc, event_rate=0.35, seed=431,
-                            nthreads=8)
-    surv = out["values"].sum(axis=1)
-    assert np.max(np.abs(surv - np.exp(-0.2 * times))) < 2e-6
-    H, K = _pair_density_inputs(system)
+    direct = h.st_dephasing_direct(system, times)
+    for method, kry in ((0, 8), (1, 8), (2, 8)):  # Krylov, dense exponential, RK4
+        out = orc.hs_stochastic(Hc, F, times, obs, kappa=0.1, krylov=kry, method=method, U_csr=Uc, event_rate=0.35,
+                                seed=431, nthreads=8)
+        assert out["values"].shape == (81, 4)
+        err = den.data_file_difference(out["values"], direct)
+        assert abs(err - h.ST_DEPHASING_POPULATION_ERROR) < h.ST_DEPHASING_PIN_TOL, (method, err)
+        assert err < h.six_sigma(M)  # check_output.py's own bound
+        surv = np.max(np.abs(out["values"].sum(axis=1) - np.exp(-0.2 * times)))
+        # reference (autoexpm): 8.129053e-13; RK4 adds its own truncation of e^{-kt}
+        assert surv < (2e-10 if method == 2 else 1e-11), (method, surv)
+
+
+def test_st_dephasing_direct_arm_is_the_lindblad_dynamics():
+    # The direct arm's RK4 at dt 0.025 agrees with the exact Lindblad exponential far below
+    # the pin's tolerance, and the coherent (no-ST) answer is far away, so the check has teeth
+    # (the reference's fixture checks the latter at 0.07, Tests/tests_StochasticRelaxation.cpp:197-217).
+    system = h.st_fixture()
+    times = orc.time_grid(2.0, 0.025)
+    direct = h.st_dephasing_direct(system, times)
+    H = den.dense_hamiltonian(system)
+    K = 0.1 * np.eye(system.dim)
     rho0 = den.singlet_density(system)
-    ops = [(den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), system), 1.0) for n in ("S", "T0", "Tp", "Tm")]
-    # the reference's "direct" arm: exact Lindblad dynamics at every grid point
-    direct = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t, den.st_unitary(system), 0.7)).real
-                        for O, _ in ops] for t in times])
-    err = np.max(np.abs(out["values"] - direct))
-    assert err < h.six_sigma(M), err
-    # the coherent (no-ST) direct answer is far away, so the check has teeth
-    coherent = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t)).real for O, _ in ops] for t in times])
-    assert abs(direct[-1, 0] - coherent[-1, 0]) > 0.07
+    ops = [den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), system) for n in ("S", "T0", "Tp", "Tm")]
+    exact = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t, den.st_unitary(system), 0.7)).real
+                       for O in ops] for t in times])
+    assert np.max(np.abs(direct - exact)) < 1e-8
+    coherent = np.array([[np.trace(O @ den.lindblad_exact(H, K, rho0, t)).real for O in ops] for t in times])
+    assert abs(exact[-1, 0] - coherent[-1, 0]) > 0.07
 
 
 def test_split_second_order():

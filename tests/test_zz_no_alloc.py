@@ -59,8 +59,9 @@ def test_noalloc_step_matches_regular_entry_point_twice():
         assert err < 1e-12, f"call {call}: relative deviation {err:.3e}"
         psi = got
 
-    # a problem larger than the static scratch area is refused before any work
-    big = 1 << 16
-    rc = L.lib.msgpu_krylov_step_noalloc(D, d_row.data_ptr(), d_col.data_ptr(), d_val.data_ptr(), kappa, big,
-                                         d_in.data_ptr(), d_out.data_ptr(), dt, m, stream.cuda_stream)
-    assert rc == L.MSGPU_ERR_SCRATCH
+    # problems larger than the static scratch area are refused before any
+    # work, the largest trajectory count included (no index overflow)
+    for big in (1 << 16, 2 ** 31 - 1):
+        rc = L.lib.msgpu_krylov_step_noalloc(D, d_row.data_ptr(), d_col.data_ptr(), d_val.data_ptr(), kappa, big,
+                                             d_in.data_ptr(), d_out.data_ptr(), dt, m, stream.cuda_stream)
+        assert rc == L.MSGPU_ERR_SCRATCH, (big, rc)
