@@ -82,8 +82,12 @@ extern "C" {
                                         variant and tile; k >= 0: tune the tile of variant k
                                         only (0-3 register-gather variants, 4-5 the variants
                                         that stage the tile's own quartets in shared memory,
-                                        6-7 two trajectory pairs per thread); a forced variant
-                                        also keeps the four-kernel Lanczos iteration */
+                                        6-7 two trajectory pairs per thread, 8-9 the
+                                        tensor-core SpMM over cubes of 16 / 8 quartets, for
+                                        radical pairs whose other spins are all spin-1/2;
+                                        refused with MSGPU_ERR_INVALID at the run otherwise);
+                                        a forced variant also keeps the four-kernel Lanczos
+                                        iteration */
 #define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
                                         (default, "double"), 2^-24 ("single"), 2^-10 ("half") */
 #define MSGPU_OPT_LANCZOS_CLUSTER 4   /* complex64 streamed form.  0 (default): per Krylov

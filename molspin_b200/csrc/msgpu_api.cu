@@ -17,6 +17,7 @@
 #include "msgpu_fused.cuh"
 #include "msgpu_kernels.cuh"
 #include "msgpu_resident.cuh"
+#include "msgpu_spmm_tc.cuh"
 
 using namespace msgpu;
 
@@ -26,7 +27,8 @@ enum KClass {
     KC_APPLY = 0, KC_ORTH = 1, KC_REDUCE = 2, KC_EXPM = 3, KC_COMBINE = 4, KC_YIELD = 5, KC_GEMM = 6, KC_LANCZOS = 7,
     KC_N = 8
 };
-constexpr int kNumSpmmVariants = 8;  // entries of kApplyVariants (checked there)
+constexpr int kNumSimtVariants = 8;  // entries of kApplyVariants (checked there)
+constexpr int kNumSpmmVariants = kNumSimtVariants + 2;  // + the tensor-core SpMM, cube bits 4 and 3
 
 struct DevBuf {
     void *p = nullptr;
@@ -79,6 +81,12 @@ struct msgpu_ctx {
     // evaluated by the caller at each step's midpoint
     std::vector<double> sched;
     long long sched_first = 0, sched_steps = 0;
+    // tensor-core SpMM (k_lanczos_apply_tc): B-operand tables of the quartet
+    // form, built when the quartet form has the nuclear-bit structure
+    DevBuf tc_src, tc_tab;
+    int tc_P = 0, tc_entries = 0;
+    long long tc_build = -1;   // quartet build the tables were validated for
+    bool tc_ok = false;        // structure present (tables valid)
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
     int q_variant = 0;               // autotuned kernel variant (kApplyVariants)
     // resident (one warp per trajectory, whole time loop per launch) form
@@ -314,7 +322,7 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
                      &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d,
-                     &c->dense_part, &c->hterms, &c->qsrc};
+                     &c->dense_part, &c->hterms, &c->qsrc, &c->tc_src, &c->tc_tab};
     for (DevBuf *b : all) release(c, *b);
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -1009,6 +1017,17 @@ int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
 }
 
 // Quartet-block form of H for the current electron strides (see QuartetC).
+// B-operand tables of the tensor-core SpMM from the current quartet values.
+int tc_tables(msgpu_ctx *c)
+{
+    if (!c->tc_ok) return MSGPU_OK;
+    k_tc_tables<<<c->tc_entries, 256, 0, c->stream>>>(static_cast<const int2 *>(c->tc_src.p), c->tc_entries,
+                                                      static_cast<const float4 *>(c->qval.p),
+                                                      static_cast<unsigned char *>(c->tc_tab.p));
+    const cudaError_t e = cudaGetLastError();
+    return e ? cuda_fail(c, e, "tensor-core SpMM tables") : MSGPU_OK;
+}
+
 int refresh_quartet_values(msgpu_ctx *c)
 {
     if (!c->q_nslots) return MSGPU_OK;
@@ -1016,7 +1035,8 @@ int refresh_quartet_values(msgpu_ctx *c)
         static_cast<const int *>(c->qsrc.p), c->q_nslots, static_cast<const double2 *>(c->hval.p),
         static_cast<float2 *>(c->qval.p));
     const cudaError_t e = cudaGetLastError();
-    return e ? cuda_fail(c, e, "quartet value refresh") : MSGPU_OK;
+    if (e) return cuda_fail(c, e, "quartet value refresh");
+    return c->tc_build == c->q_build ? tc_tables(c) : MSGPU_OK;
 }
 
 int build_quartet(msgpu_ctx *c)
@@ -1157,6 +1177,112 @@ QuartetC quartet_view(const msgpu_ctx *c)
     return QuartetC{static_cast<const int *>(c->qrow.p), static_cast<const int2 *>(c->qcolt.p),
                     static_cast<const float4 *>(c->qval.p), static_cast<const int *>(c->qbase.p)};
 }
+
+// Validates the nuclear-bit structure the tensor-core SpMM relies on, on the
+// host copy of the quartet form: Q = 2^P quartets, every block couples q to
+// itself or to q ^ 2^p, every quartet has the same set of flip bits, and the
+// flip block of (p, bit p of the output quartet) is the same in every quartet.
+// Then builds the table entries (2P flip entries, then Q diagonal entries) and
+// the B-operand tables.  tc_ok stays false when the structure is absent.
+int build_tc(msgpu_ctx *c)
+{
+    if (c->tc_build == c->q_build) return MSGPU_OK;
+    c->tc_build = c->q_build;
+    c->tc_ok = false;
+    const int Q = c->D / 4, s1 = c->s1, s2 = c->s2;
+    int P = 0;
+    while ((1 << P) < Q) ++P;
+    if ((1 << P) != Q || P < 5 || P > kTcMaxBits) return MSGPU_OK;
+    // quartet index of a base row (inverse of the base map of build_quartet)
+    auto qindex = [&](int b) {
+        const int lo = b % s2, mid = (b / (2 * s2)) % (s1 / (2 * s2)), hi = b / (2 * s1);
+        return hi * (s1 / 2) + mid * s2 + lo;
+    };
+    // full 4 x 4 complex block of a compact entry (host twin of tc_expand)
+    auto expand = [&](int type, int off, std::array<float, 32> &h) {
+        h.fill(0.f);
+        const float *v = c->q_hval.data() + 4 * static_cast<size_t>(off);
+        auto set = [&](int a, int b, int i) {
+            h[2 * (4 * a + b)] = v[2 * i];
+            h[2 * (4 * a + b) + 1] = v[2 * i + 1];
+        };
+        switch (type) {
+        case 0:
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b) set(a, b, 4 * a + b);
+            break;
+        case 1:
+            for (int a2 = 0; a2 < 2; ++a2)
+                for (int a1 = 0; a1 < 2; ++a1)
+                    for (int b1 = 0; b1 < 2; ++b1) set(2 * a1 + a2, 2 * b1 + a2, (2 * a2 + a1) * 2 + b1);
+            break;
+        case 2:
+            for (int a1 = 0; a1 < 2; ++a1)
+                for (int a2 = 0; a2 < 2; ++a2)
+                    for (int b2 = 0; b2 < 2; ++b2) set(2 * a1 + a2, 2 * a1 + b2, (2 * a1 + a2) * 2 + b2);
+            break;
+        case 3:
+            for (int a = 0; a < 4; ++a) set(a, a, a);
+            break;
+        case 4:
+            for (int a1 = 0; a1 < 2; ++a1)
+                for (int b1 = 0; b1 < 2; ++b1)
+                    for (int a2 = 0; a2 < 2; ++a2) set(2 * a1 + a2, 2 * b1 + a2, 2 * a1 + b1);
+            break;
+        default:
+            for (int a2 = 0; a2 < 2; ++a2)
+                for (int b2 = 0; b2 < 2; ++b2)
+                    for (int a1 = 0; a1 < 2; ++a1) set(2 * a1 + a2, 2 * a1 + b2, 2 * a2 + b2);
+            break;
+        }
+    };
+    const int nent = 2 * P + Q;
+    std::vector<int2> src(nent, make_int2(-1, 0));
+    std::vector<std::array<float, 32>> rep(2 * P);
+    std::vector<unsigned> mask(Q, 0u);
+    std::array<float, 32> h;
+    for (int q = 0; q < Q; ++q)
+        for (int k = c->q_hrow[q]; k < c->q_hrow[q + 1]; ++k) {
+            const int2 blk = c->q_hblk[k];
+            const int d = q ^ qindex(blk.x >> 3), type = blk.x & 7;
+            if (d == 0) {
+                src[2 * P + q] = make_int2(blk.y, type);
+                continue;
+            }
+            if (d & (d - 1)) return MSGPU_OK;  // not a single nuclear flip
+            int p = 0;
+            while ((1 << p) != d) ++p;
+            mask[q] |= 1u << p;
+            const int e = 2 * p + ((q >> p) & 1);
+            expand(type, blk.y, h);
+            if (src[e].x < 0) {
+                src[e] = make_int2(blk.y, type);
+                rep[e] = h;
+                continue;
+            }
+            float amax = 0.f, dmax = 0.f;
+            for (int i = 0; i < 32; ++i) {
+                amax = std::max(amax, std::abs(rep[e][i]));
+                dmax = std::max(dmax, std::abs(rep[e][i] - h[i]));
+            }
+            if (dmax > 0x1p-22f * amax) return MSGPU_OK;  // the flip block depends on more than (p, bit)
+        }
+    for (int q = 1; q < Q; ++q)
+        if (mask[q] != mask[0]) return MSGPU_OK;
+    int rc;
+    if ((rc = ensure(c, c->tc_src, sizeof(int2) * nent, "tensor-core SpMM table entries")) ||
+        (rc = ensure(c, c->tc_tab, static_cast<size_t>(nent) * 3 * kTcB, "tensor-core SpMM tables")))
+        return rc;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(c->tc_src.p, src.data(), sizeof(int2) * nent, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_fail(c, e, "tensor-core SpMM table entries");
+    c->tc_P = P;
+    c->tc_entries = nent;
+    c->tc_ok = true;
+    return tc_tables(c);
+}
+
 
 // ------------------------------------------------- cluster-resident Lanczos
 // Bound on the off-diagonal blocks one CTA of k_lanczos_fused<C> stages (the
@@ -1387,13 +1513,48 @@ const ApplyVariant kApplyVariants[] = {
     {k_lanczos_apply_np<2, 3>, false, 2},
 };
 constexpr int kNumApplyVariants = sizeof(kApplyVariants) / sizeof(kApplyVariants[0]);
-static_assert(kNumApplyVariants == kNumSpmmVariants, "SpMM variant count");
+static_assert(kNumApplyVariants == kNumSimtVariants, "SpMM variant count");
 constexpr int kCubeMaxQT = 64;  // 128 KB of shared memory
+// Whether the tensor-core SpMM (variants kNumSimtVariants + 0 / + 1: cube bits
+// 4 / 3) takes part in the tuner's choice; it can always be forced with
+// MSGPU_OPT_SPMM_VARIANT.
+constexpr bool kTcInTuner = false;
+
+int tc_cube_bits(int v) { return v == kNumSimtVariants ? 4 : 3; }
+
+// U = s H w over `width` trajectories with the tensor-core SpMM.
+void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, const double *s, float2 *U, double *part,
+               int width)
+{
+    const int Q = c->D / 4, P = c->tc_P;
+    const unsigned char *tflip = static_cast<const unsigned char *>(c->tc_tab.p);
+    const unsigned char *tdiag = tflip + static_cast<size_t>(2 * P) * 3 * kTcB;
+    const dim3 grid(Q >> cb, ceil_div(width, kTcTraj));
+    int *status = static_cast<int *>(c->status.p);
+    const int *base = static_cast<const int *>(c->qbase.p);
+    if (cb == 4) {
+        const int smem = TcCfg<4>::smem(P);
+        cudaFuncSetAttribute(k_lanczos_apply_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_lanczos_apply_tc<4><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
+                                                              width, status);
+    } else {
+        const int smem = TcCfg<3>::smem(P);
+        cudaFuncSetAttribute(k_lanczos_apply_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_lanczos_apply_tc<3><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
+                                                              width, status);
+    }
+}
 
 // Whether variant v can run with tile QT on this system, and its shared memory.
 bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 {
     *smem = 0;
+    if (v >= kNumSimtVariants) {
+        const int cb = tc_cube_bits(v);
+        if (!c->tc_ok || qt != (1 << cb) || c->tc_P < cb + 1) return false;
+        *smem = static_cast<size_t>(cb == 4 ? TcCfg<4>::smem(c->tc_P) : TcCfg<3>::smem(c->tc_P));
+        return true;
+    }
     // the step launches it over one trajectory group, the tuner over the whole block
     if ((c->ldm / traj_groups(c)) % (64 * kApplyVariants[v].np) != 0 || c->ldm % (64 * kApplyVariants[v].np) != 0)
         return false;
@@ -1408,6 +1569,10 @@ bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st, const float2 *w, const double *s,
                   float2 *U, double *part, int width)
 {
+    if (v >= kNumSimtVariants) {
+        launch_tc(c, tc_cube_bits(v), st, w, s, U, part, width);
+        return;
+    }
     size_t smem = 0;
     apply_fits(c, v, qt, &smem);
     grid.y = width / (64 * kApplyVariants[v].np);
@@ -1429,8 +1594,9 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
     // pick the shape
     std::vector<std::pair<int, int>> cands;
     size_t smem;
-    for (int v = 0; v < kNumApplyVariants; ++v) {
+    for (int v = 0; v < kNumSpmmVariants; ++v) {
         if (c->spmm_variant >= 0 && v != c->spmm_variant) continue;
+        if (c->spmm_variant < 0 && v >= kNumSimtVariants && !kTcInTuner) continue;
         for (int qt : cand)
             if ((qt <= Q || qt == cand[0]) && apply_fits(c, v, qt, &smem)) cands.push_back({v, qt});
     }
@@ -1721,6 +1887,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     int fused_c = 0;  // cluster size of k_lanczos_fused, 0: the four-kernel iteration
     if (prec == MSGPU_PREC_C64) {
         if (int rc = build_quartet(c)) return rc;
+        if (int rc = build_tc(c)) return rc;
         fused_c = fused_cluster(c);
         if (!fused_c)
             if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc,
@@ -2001,6 +2168,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     collect_profile(c);
     c->last_ntimes = p->ntimes;
     c->have_integrals = true;
+    if (status & 4) return fail(c, MSGPU_ERR_CUDA, "run: tensor-core SpMM pipeline timed out (bounded wait expired)");
     if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite observable or norm on the device");
     if (status & 1) return fail(c, MSGPU_ERR_EXPM, "run: small matrix exponential failed");
     return MSGPU_OK;

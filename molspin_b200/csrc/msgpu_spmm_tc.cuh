@@ -1,0 +1,509 @@
+// msgpu_spmm_tc.cuh -- quartet SpMM of the complex64 Lanczos form on the
+// 5th-generation tensor cores (tcgen05, TMEM, TMA bulk copies).
+//
+// U = s_j H w_j over a trajectory block (the H v product of
+// SpinSpace::LanczosProcess / ArnoldiProcess, SpinSpace_operators.cpp:1362,
+// applied per column by HSPropagator::Step, HSPropagator.cpp:64-78).
+//
+// Structure used.  For radical pairs whose other spins are all spin-1/2, the
+// quartet index q (the row index with the two electron digits removed) is a
+// P-bit number, one bit per nucleus, and H couples quartet q only to itself
+// (a 4x4 diagonal block that depends on q) and to q ^ 2^p (one block per
+// nucleus p that depends only on p and on bit p of the output quartet).  The
+// host checks this on the quartet form before it enables the kernel.
+//
+// Work split.  A CTA owns a cube of 2^CB output quartets (the low CB bits
+// free, the high bits fixed) for 128 trajectories.  Its inputs are the cube
+// itself (each input feeds its own output and CB in-cube flips) and, for
+// every nucleus p >= CB, the translated cube q ^ 2^p (each input feeds one
+// output).  Every input quartet is loaded once per CTA and feeds all of the
+// CTA's outputs that need it through the tensor cores: 1 + P - CB loads per
+// output quartet against 1 + P in the SIMT kernels, whose limit is the L1
+// data path.
+//
+// Data path per input quartet (4 rows x 128 trajectories, complex64,
+// pair-planar): TMA bulk copies (one 1 KB row each) into shared memory;
+// 128 producer threads (thread = trajectory = TMEM lane) read their 8 real
+// values (Re/Im of the 4 rows), split each into three BF16 parts
+// x = x0 + x1 + x2 and store [x0 | x1 | x0 | x2] (16 TMEM columns) into a
+// TMEM slot; one thread issues, per (output, input) pair, three
+// tcgen05.mma kind::f16 (M = 128 trajectories, N = 16, K = 16, A from TMEM,
+// B = the block in real form from shared memory):
+//     D_main += [x0 | x1] . [H0 ; H1]        (x0 H0 + x1 H1)
+//     D_corr += [x0 | x1] . [H1 ; H0]        (x0 H1 + x1 H0)
+//     D_corr += [x0 | x2] . [H2 ; H0]        (x0 H2 + x2 H0)
+// with H = H0 + H1 + H2 the BF16 split of the block's real form (8 x 8:
+// [[Re H, -Im H], [Im H, Re H]] acting on [Re x ; Im x]).  The dropped
+// products are 2^-24 of the result.  The correction products accumulate
+// apart from the main one: the FP32 accumulation of tcgen05.mma rounds
+// towards zero, and keeping the 2^-8-sized corrections out of the main
+// accumulator limits that bias to the main products' own.  The epilogue adds
+// the two accumulators (round to nearest), scales by s_j, stores U and the
+// per-trajectory FP64 partial of alpha_j = Re <v_j, U>.
+//
+// TMEM columns (CB = 4, 512 allocated): D_main [0, 128) + 8 pad, D_corr
+// [136, 264) + 8 pad, then 15 input slots of 16 columns.  An MMA of N = 16
+// writing an output's 8 columns also covers the next 8 (the B operand's
+// columns 8..15 are zero), hence the pads; the accumulators are cleared once
+// and every MMA accumulates.  CB = 3 allocates 256 columns (two CTAs per SM).
+//
+// Every mbarrier wait is bounded; after the limit the kernel records status
+// bit 4, lets its own copies and MMAs drain (bounded), frees TMEM and
+// returns.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+namespace msgpu {
+
+constexpr int kTcTraj = 128;            // trajectories per CTA (TMEM lanes, MMA M)
+constexpr int kTcThreads = 192;         // warps 0-3 producers/epilogue, 4 MMA issuer, 5 TMA issuer
+constexpr int kTcB = 512;               // bytes of one 16 x 16 BF16 B operand
+constexpr int kTcMaxBits = 14;          // quartet bits P (D <= 65536)
+constexpr uint32_t kTcWait = 1u << 23;  // iterations of a bounded mbarrier wait
+
+template <int CB>
+struct TcCfg {
+    static constexpr int NQ = 1 << CB;             // output quartets per CTA
+    static constexpr int Cols = CB == 4 ? 512 : 256;
+    static constexpr int DMain = 0;
+    static constexpr int DCorr = 8 * NQ + 8;
+    static constexpr int Slot0 = 2 * (8 * NQ + 8);
+    static constexpr int NS = (Cols - Slot0) / 16;   // TMEM input slots
+    static constexpr int NSTG = CB == 4 ? 12 : 8;    // shared-memory stages for translated inputs
+    static constexpr int InBytes = 4 * kTcTraj * 8;  // one input quartet, 128 trajectories (4 KB)
+    // shared memory: own cube | stage ring | diagonal B operands | flip B operands (P bits) | barriers
+    static constexpr int OffOwn = 0;
+    static constexpr int OffStage = OffOwn + NQ * InBytes;
+    static constexpr int OffDiag = OffStage + NSTG * InBytes;
+    static constexpr int OffFlip = OffDiag + NQ * 3 * kTcB;
+    static constexpr int NBar = 2 + 2 * NSTG + 2 * NS + 1;  // own, tables, stage full/empty, slot full/empty, done
+    __host__ __device__ static constexpr int off_bar(int P) { return OffFlip + P * 2 * 3 * kTcB; }
+    __host__ __device__ static constexpr int smem(int P) { return off_bar(P) + NBar * 8 + 16 /*abort, tmem slot*/; }
+    static_assert(NS >= 4, "TMEM slots");
+};
+
+__device__ __forceinline__ uint32_t tc_smem(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool tc_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after the limit (the abort flag is then set) or when
+// another role aborted.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, volatile int *abort)
+{
+    for (uint32_t it = 0; it < kTcWait; ++it) {
+        if (tc_try(bar, parity)) return true;
+        if (*abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+__device__ __forceinline__ void tc_bulk(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_expect(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tc_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// B operand descriptor: K-major, no swizzle, core matrices of 8 rows x 16 B;
+// LBO = 128 B (the next 8 K), SBO = 256 B (the next 8 N rows), version 1.
+__device__ __forceinline__ uint64_t tc_bdesc(uint32_t addr)
+{
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (static_cast<uint64_t>(128 >> 4) << 16) |
+           (static_cast<uint64_t>(256 >> 4) << 32) | (static_cast<uint64_t>(1) << 46);
+}
+
+// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major, M = 128, N = 16.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(16 >> 3) << 17) |
+                              (static_cast<uint32_t>(128 >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+        :
+        : "r"(d), "r"(a), "l"(b), "r"(kTcIdesc), "r"(1u)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_st16(uint32_t taddr, const uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+
+// Byte offset of element (n, k) in a 16 x 16 BF16 B operand (see tc_bdesc).
+__host__ __device__ constexpr int tc_boff(int n, int k) { return (n >> 3) * 256 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2; }
+
+__device__ __forceinline__ uint32_t tc_pack(__nv_bfloat16 lo, __nv_bfloat16 hi)
+{
+    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// Full 4x4 complex block from the compact quartet form (the types of QuartetC).
+__device__ __forceinline__ void tc_expand(int type, const float2 *__restrict__ v, float2 (&h)[4][4])
+{
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) h[a][b] = make_float2(0.f, 0.f);
+    switch (type) {
+    case 0:
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) h[a][b] = v[4 * a + b];
+        break;
+    case 1:  // digit 1, a2 == b2: [a2][a1][b1]
+        for (int a2 = 0; a2 < 2; ++a2)
+            for (int a1 = 0; a1 < 2; ++a1)
+                for (int b1 = 0; b1 < 2; ++b1) h[2 * a1 + a2][2 * b1 + a2] = v[(2 * a2 + a1) * 2 + b1];
+        break;
+    case 2:  // digit 2, a1 == b1: [a1][a2][b2]
+        for (int a1 = 0; a1 < 2; ++a1)
+            for (int a2 = 0; a2 < 2; ++a2)
+                for (int b2 = 0; b2 < 2; ++b2) h[2 * a1 + a2][2 * a1 + b2] = v[(2 * a1 + a2) * 2 + b2];
+        break;
+    case 3:
+        for (int a = 0; a < 4; ++a) h[a][a] = v[a];
+        break;
+    case 4:  // A (x) I on digit 1: [a1][b1]
+        for (int a1 = 0; a1 < 2; ++a1)
+            for (int b1 = 0; b1 < 2; ++b1)
+                for (int a2 = 0; a2 < 2; ++a2) h[2 * a1 + a2][2 * b1 + a2] = v[2 * a1 + b1];
+        break;
+    default:  // I (x) A on digit 2: [a2][b2]
+        for (int a2 = 0; a2 < 2; ++a2)
+            for (int b2 = 0; b2 < 2; ++b2)
+                for (int a1 = 0; a1 < 2; ++a1) h[2 * a1 + a2][2 * a1 + b2] = v[2 * a2 + b2];
+        break;
+    }
+}
+
+// B-operand tables.  Entry e (src[e] = {value offset in float4 units, type} of
+// a block of the quartet form; offset < 0: no block, a zero operand) becomes
+// three 16 x 16 BF16 B operands (B1 = [H0; H1], B2 = [H1; H0], B3 = [H2; H0])
+// of the block's real form R[k][n]: k < 4 Re x_k, 4 <= k < 8 Im x_{k-4};
+// n < 4 Re y_n, 4 <= n < 8 Im y_{n-4}; columns 8..15 are zero.  One block of
+// 256 threads per entry, thread (n, k).
+__global__ void __launch_bounds__(256) k_tc_tables(const int2 *__restrict__ src, int nentries,
+                                                   const float4 *__restrict__ qval, unsigned char *__restrict__ out)
+{
+    const int e = blockIdx.x;
+    if (e >= nentries) return;
+    const int n = threadIdx.x >> 4, k = threadIdx.x & 15;
+    float r = 0.f;
+    const int2 s = src[e];
+    if (n < 8 && s.x >= 0) {
+        float2 h[4][4];
+        tc_expand(s.y, reinterpret_cast<const float2 *>(qval + s.x), h);
+        const int kk = k & 7, b = kk & 3, a = n & 3;
+        const float2 hab = h[a][b];
+        if (kk < 4) r = n < 4 ? hab.x : hab.y;  // Re x_b -> Re y_a: Re H; -> Im y_a: Im H
+        else r = n < 4 ? -hab.y : hab.x;        // Im x_b -> Re y_a: -Im H; -> Im y_a: Re H
+    }
+    const __nv_bfloat16 p0 = __float2bfloat16_rn(r);
+    const float r1 = r - __bfloat162float(p0);
+    const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
+    const bool lo = k < 8;
+    unsigned char *o = out + static_cast<size_t>(e) * 3 * kTcB + tc_boff(n, k);
+    *reinterpret_cast<__nv_bfloat16 *>(o) = lo ? p0 : p1;             // B1 = [H0; H1]
+    *reinterpret_cast<__nv_bfloat16 *>(o + kTcB) = lo ? p1 : p0;      // B2 = [H1; H0]
+    *reinterpret_cast<__nv_bfloat16 *>(o + 2 * kTcB) = lo ? p2 : p0;  // B3 = [H2; H0]
+}
+
+// U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
+// kTcThreads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
+//   tflip: [P][2 (output bit)][3] B operands; tdiag: [Q][3] B operands;
+//   base: quartet -> base row; {0, s2, s1, s1 + s2}: the rows of a quartet;
+//   w, sj, U, part start at the group's first trajectory; width = its
+//   trajectories (a multiple of 64); ldm = the row stride.
+template <int CB>
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char *__restrict__ tdiag, int P,
+                   const int *__restrict__ base, int s1, int s2, const float2 *__restrict__ w,
+                   const double *__restrict__ sj, float2 *__restrict__ U, double *__restrict__ part, int ldm,
+                   int width, int *__restrict__ status)
+{
+    using Cfg = TcCfg<CB>;
+    constexpr int NQ = Cfg::NQ, NS = Cfg::NS, NSTG = Cfg::NSTG;
+    extern __shared__ __align__(128) unsigned char tc_raw[];
+    unsigned char *sm = tc_raw;
+    const uint32_t sbase = tc_smem(sm);
+    const uint32_t bar0 = sbase + Cfg::off_bar(P);
+    const uint32_t bar_own = bar0, bar_tab = bar0 + 8;
+    auto bar_sfull = [&](int s) { return bar0 + 16 + 8 * s; };
+    auto bar_sempty = [&](int s) { return bar0 + 16 + 8 * (NSTG + s); };
+    auto bar_tfull = [&](int s) { return bar0 + 16 + 8 * (2 * NSTG + s); };
+    auto bar_tempty = [&](int s) { return bar0 + 16 + 8 * (2 * NSTG + NS + s); };
+    const uint32_t bar_done = bar0 + 16 + 8 * (2 * NSTG + 2 * NS);
+    volatile int *abort = reinterpret_cast<volatile int *>(sm + Cfg::off_bar(P) + Cfg::NBar * 8);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Cfg::off_bar(P) + Cfg::NBar * 8 + 8);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int cube = blockIdx.x, q0 = cube << CB;
+    const int t0 = blockIdx.y * kTcTraj;          // first trajectory of the tile (in the group)
+    const int nvalid = min(kTcTraj, width - t0);  // a multiple of 64 (width is)
+    const int NI = NQ * (1 + P - CB);             // input quartets
+    const int off[4] = {0, s2, s1, s1 + s2};
+
+    if (tid == 0) {
+        *abort = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_own));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_tab));
+        for (int s = 0; s < NSTG; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_sfull(s)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_sempty(s)), "r"(4));
+        }
+        for (int s = 0; s < NS; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_tfull(s)), "r"(4));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_tempty(s)));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_done));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(tslot)),
+                     "r"(Cfg::Cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+
+    // input j -> quartet (global index): the own cube, then one translated cube per nucleus p >= CB
+    auto input_quartet = [&](int j) {
+        const int g = j >> CB, l = j & (NQ - 1);
+        return g == 0 ? q0 + l : (q0 + l) ^ (1 << (CB + g - 1));
+    };
+
+    if (warp == 5) {
+        // ------------------------------------------------------------ TMA issuer
+        if (tid == 160) {
+            const uint32_t rowbytes = static_cast<uint32_t>(nvalid) * 8u;
+            // B operands: every flip entry and this cube's diagonal blocks
+            tc_expect(bar_tab, static_cast<uint32_t>((P * 2 + NQ) * 3 * kTcB));
+            tc_bulk(sbase + Cfg::OffFlip, tflip, static_cast<uint32_t>(P * 2 * 3 * kTcB), bar_tab);
+            tc_bulk(sbase + Cfg::OffDiag, tdiag + static_cast<size_t>(q0) * 3 * kTcB,
+                    static_cast<uint32_t>(NQ * 3 * kTcB), bar_tab);
+            // the own cube: NQ quartets x 4 rows, kept for the alpha partial
+            tc_expect(bar_own, static_cast<uint32_t>(NQ * 4) * rowbytes);
+            for (int l = 0; l < NQ; ++l) {
+                const int b = base[q0 + l];
+                for (int a = 0; a < 4; ++a)
+                    tc_bulk(sbase + Cfg::OffOwn + (l * 4 + a) * kTcTraj * 8, w + static_cast<size_t>(b + off[a]) * ldm + t0,
+                            rowbytes, bar_own);
+            }
+            // translated cubes through the stage ring
+            int issued = 0;
+            for (int j = NQ; j < NI && !*abort; ++j) {
+                const int k = j - NQ, s = k % NSTG, r = k / NSTG;
+                if (!tc_wait(bar_sempty(s), (r & 1) ^ 1, abort)) break;
+                tc_expect(bar_sfull(s), 4u * rowbytes);
+                const int b = base[input_quartet(j)];
+                for (int a = 0; a < 4; ++a)
+                    tc_bulk(sbase + Cfg::OffStage + s * Cfg::InBytes + a * kTcTraj * 8,
+                            w + static_cast<size_t>(b + off[a]) * ldm + t0, rowbytes, bar_sfull(s));
+                issued = k + 1;
+            }
+            // every copy this CTA started lands before the CTA can exit
+            for (int k = max(0, issued - NSTG); k < issued; ++k)
+                for (uint32_t it = 0; it < kTcWait && !tc_try(bar_sfull(k % NSTG), (k / NSTG) & 1); ++it) {
+                }
+            for (uint32_t it = 0; it < kTcWait && !tc_try(bar_own, 0); ++it) {
+            }
+            for (uint32_t it = 0; it < kTcWait && !tc_try(bar_tab, 0); ++it) {
+            }
+        }
+    } else if (warp == 4) {
+        // ------------------------------------------------------------ MMA issuer
+        if (tid == 128) {
+            bool ok = tc_wait(bar_tab, 0, abort);
+            const uint32_t flip_s = sbase + Cfg::OffFlip, diag_s = sbase + Cfg::OffDiag;
+            for (int j = 0; j < NI && ok; ++j) {
+                const int s = j % NS, r = j / NS;
+                if (!tc_wait(bar_tfull(s), r & 1, abort)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a01 = tmem + Cfg::Slot0 + 16 * s, a02 = a01 + 8;
+                const int g = j >> CB, l = j & (NQ - 1);
+                auto issue = [&](int o, uint32_t bt) {
+                    const uint32_t dm = tmem + Cfg::DMain + 8 * o, dc = tmem + Cfg::DCorr + 8 * o;
+                    tc_mma(dm, a01, tc_bdesc(bt));
+                    tc_mma(dc, a01, tc_bdesc(bt + kTcB));
+                    tc_mma(dc, a02, tc_bdesc(bt + 2 * kTcB));
+                };
+                if (g == 0) {
+                    issue(l, diag_s + l * 3 * kTcB);  // own block
+#pragma unroll
+                    for (int p = 0; p < CB; ++p) {
+                        const int o = l ^ (1 << p);
+                        issue(o, flip_s + ((p * 2 + ((o >> p) & 1)) * 3) * kTcB);
+                    }
+                } else {
+                    const int p = CB + g - 1;
+                    issue(l, flip_s + ((p * 2 + ((q0 >> p) & 1)) * 3) * kTcB);
+                }
+                tc_commit(bar_tempty(s));
+            }
+            tc_commit(bar_done);  // completes once every MMA issued above has
+        }
+    } else {
+        // ------------------------------------------------------------ producers
+        const int lane_traj = tid;                  // TMEM lane = trajectory in the tile
+        const int pair_off = (lane_traj & ~1) * 8;  // byte offset of the trajectory pair in a row
+        const bool odd = lane_traj & 1;
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(32 * warp) << 16);
+        // clear both accumulators and their pads (every MMA accumulates); the
+        // first slot's fence and arrive below order this before any MMA
+        {
+            uint32_t z[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[i] = 0u;
+            for (int c0 = 0; c0 < Cfg::Slot0; c0 += 16) tc_st16(lane_addr + c0, z);
+        }
+        // every wait's outcome is made uniform over the warp: the tcgen05.st/ld
+        // and the shuffles below are warp-collective
+        bool ok = __all_sync(0xffffffffu, tc_wait(bar_own, 0, abort));
+        for (int j = 0; j < NI && ok; ++j) {
+            const unsigned char *src;
+            if (j < NQ) {
+                src = sm + Cfg::OffOwn + j * Cfg::InBytes;
+            } else {
+                const int k = j - NQ;
+                if (!__all_sync(0xffffffffu, tc_wait(bar_sfull(k % NSTG), (k / NSTG) & 1, abort))) {
+                    ok = false;
+                    break;
+                }
+                src = sm + Cfg::OffStage + (k % NSTG) * Cfg::InBytes;
+            }
+            float x[8];  // Re rows 0..3, Im rows 0..3
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const float4 v = *reinterpret_cast<const float4 *>(src + a * kTcTraj * 8 + pair_off);
+                x[a] = odd ? v.y : v.x;
+                x[4 + a] = odd ? v.w : v.z;
+            }
+            if (j >= NQ) {
+                __syncwarp();
+                if ((tid & 31) == 0) tc_arrive(bar_sempty((j - NQ) % NSTG));
+            }
+            uint32_t pk[16];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                __nv_bfloat16 h0[2], h1[2], h2[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const float xv = x[2 * c + e];
+                    h0[e] = __float2bfloat16_rn(xv);
+                    const float r1 = xv - __bfloat162float(h0[e]);
+                    h1[e] = __float2bfloat16_rn(r1);
+                    h2[e] = __float2bfloat16_rn(r1 - __bfloat162float(h1[e]));
+                }
+                pk[c] = tc_pack(h0[0], h0[1]);
+                pk[4 + c] = tc_pack(h1[0], h1[1]);
+                pk[8 + c] = pk[c];
+                pk[12 + c] = tc_pack(h2[0], h2[1]);
+            }
+            const int s = j % NS, r = j / NS;
+            if (!__all_sync(0xffffffffu, tc_wait(bar_tempty(s), (r & 1) ^ 1, abort))) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            tc_st16(lane_addr + Cfg::Slot0 + 16 * s, pk);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if ((tid & 31) == 0) tc_arrive(bar_tfull(s));
+        }
+        // ------------------------------------------------------------ epilogue
+        bool done = tc_wait(bar_done, 0, abort);
+        if (!done)  // the MMA issuer commits this barrier whatever happened: let its MMAs drain
+            for (uint32_t it = 0; it < kTcWait && !tc_try(bar_done, 0); ++it) {
+            }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (__all_sync(0xffffffffu, done && ok && !*abort)) {
+            const bool live = lane_traj < nvalid;
+            const int t = t0 + lane_traj;
+            const float sc = live ? static_cast<float>(sj[t]) : 0.f;
+            double acc = 0.0;
+            for (int o = 0; o < NQ; ++o) {
+                uint32_t dm[8], dc[8];
+                tc_ld8(lane_addr + Cfg::DMain + 8 * o, dm);
+                tc_ld8(lane_addr + Cfg::DCorr + 8 * o, dc);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float y[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) y[i] = (__uint_as_float(dc[i]) + __uint_as_float(dm[i])) * sc;
+                // own input rows of this output (for alpha), pair-planar
+                const unsigned char *own = sm + Cfg::OffOwn + o * Cfg::InBytes;
+                const int b = base[q0 + o];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const float4 v = *reinterpret_cast<const float4 *>(own + a * kTcTraj * 8 + pair_off);
+                    const float vr = odd ? v.y : v.x, vi = odd ? v.w : v.z;
+                    acc += static_cast<double>(vr) * y[a] + static_cast<double>(vi) * y[4 + a];
+                    // the pair's float4 {re t, re t+1, im t, im t+1}: lanes t, t^1 exchange
+                    const float pr = __shfl_xor_sync(0xffffffffu, y[a], 1);
+                    const float pi = __shfl_xor_sync(0xffffffffu, y[4 + a], 1);
+                    if (live && ((a & 1) == static_cast<int>(odd))) {
+                        // even lanes store rows 0 and 2, odd lanes rows 1 and 3
+                        const float4 st = odd ? make_float4(pr, y[a], pi, y[4 + a]) : make_float4(y[a], pr, y[4 + a], pi);
+                        *reinterpret_cast<float4 *>(U + static_cast<size_t>(b + off[a]) * ldm + t0 + (lane_traj & ~1)) = st;
+                    }
+                }
+            }
+            if (live) part[static_cast<size_t>(cube) * ldm + t] = acc * static_cast<double>(sc);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*abort && tid == 0) atomicOr(status, 4);
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::Cols));
+    }
+}
+
+}  // namespace msgpu
