@@ -53,6 +53,8 @@ def _args():
     ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6")
     ap.add_argument("--spmm-variant", type=int, default=-1,
                     help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
+    ap.add_argument("--combine-tile", type=int, default=0,
+                    help="precision form: quartets per CTA of the combine (MSGPU_OPT_COMBINE_TILE; 0 default)")
     ap.add_argument("--lanczos-cluster", type=int, default=0,
                     help="precision form: 0 four-kernel Lanczos iteration (default); -1, 1, 2, 4, 8, 16 the "
                          "cluster-resident recurrence (MSGPU_OPT_LANCZOS_CLUSTER)")
@@ -216,6 +218,8 @@ def run_ours(args):
         p.set_option(L.OPT_SPMM_VARIANT, args.spmm_variant)
     if args.lanczos_cluster:
         p.set_option(L.OPT_LANCZOS_CLUSTER, args.lanczos_cluster)
+    if args.combine_tile:
+        p.set_option(L.OPT_COMBINE_TILE, args.combine_tile)
     p.set_hamiltonian(rowptr, col, val)
     p.set_reaction(kappa=sysm.kappa())
     p.set_electron_pair(*sysm.electron_strides())

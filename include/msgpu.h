@@ -108,6 +108,11 @@ extern "C" {
                                         memory-bound update and combine; 1: one group; 2 or 4:
                                         that many groups when each is a multiple of 128
                                         trajectories.  Results do not depend on it. */
+#define MSGPU_OPT_COMBINE_TILE 6      /* streamed forms: quartets per CTA of the evaluation and
+                                        Krylov-combination kernels (and so the number of
+                                        per-tile partial sums of the yields); 0 (default) picks
+                                        it from the dimension.  Ensemble and per-trajectory
+                                        yields change only by FP64 summation order. */
 
 /* Execution forms (msgpu_set_form).  AUTO picks RESIDENT for small
  * dimensions (the whole time loop in one launch, one warp per trajectory,

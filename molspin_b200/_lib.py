@@ -36,6 +36,7 @@ OPT_TAYLOR_TOL = 2
 OPT_SPMM_VARIANT = 3
 OPT_LANCZOS_CLUSTER = 4
 OPT_TRAJ_GROUPS = 5
+OPT_COMBINE_TILE = 6
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
 OPT_DENSE_RENORMALIZE = 1

@@ -68,6 +68,7 @@ struct msgpu_ctx {
     // complex64 streamed step in trajectory groups (MSGPU_OPT_TRAJ_GROUPS): one
     // group's SpMM overlaps the other's update and combine on a second stream
     int tgroups_opt = 0;  // 0 auto, else the number of groups asked for
+    int combine_tile_opt = 0;  // MSGPU_OPT_COMBINE_TILE: quartets per evaluation tile (0: by dimension)
     cudaStream_t gside = nullptr;
     cudaEvent_t gfork = nullptr, gjoin = nullptr;
     // H as a fixed-pattern linear combination of terms (msgpu_upload_hamiltonian_terms):
@@ -362,6 +363,12 @@ int msgpu_set_option(msgpu_ctx *c, int key, double value)
         c->q_tile = 0;  // the variants that fit depend on a group's width
         return MSGPU_OK;
     }
+    if (key == MSGPU_OPT_COMBINE_TILE) {
+        const int v = static_cast<int>(value);
+        if (v != value || v < 0 || v > 4096) return fail(c, MSGPU_ERR_INVALID, "combine tile must be 0..4096 quartets");
+        c->combine_tile_opt = v;
+        return MSGPU_OK;
+    }
     if (key == MSGPU_OPT_LANCZOS_CLUSTER) {
         const int v = static_cast<int>(value);
         if (v != value || !(v == -1 || v == 0 || v == 1 || v == 2 || v == 4 || v == 8 || v == 16))
@@ -387,6 +394,7 @@ int msgpu_get_option(msgpu_ctx *c, int key, double *value)
     case MSGPU_OPT_SPMM_VARIANT: *value = c->spmm_variant; return MSGPU_OK;
     case MSGPU_OPT_LANCZOS_CLUSTER: *value = c->f_opt; return MSGPU_OK;
     case MSGPU_OPT_TRAJ_GROUPS: *value = c->ldm ? traj_groups(c) : c->tgroups_opt; return MSGPU_OK;
+    case MSGPU_OPT_COMBINE_TILE: *value = c->combine_tile_opt; return MSGPU_OK;
     default: return fail(c, MSGPU_ERR_INVALID, "unknown option");
     }
 }
@@ -669,7 +677,8 @@ int ensure_workspace(msgpu_ctx *c, int prec, int m)
     c->rows_per_tile = pick_rows_per_tile(D);
     c->ntiles = ceil_div(D, c->rows_per_tile);
     const int Q = D / 4;
-    c->quartets_per_tile = std::max(8, std::min(256, Q / 64));
+    c->quartets_per_tile = c->combine_tile_opt > 0 ? std::min(c->combine_tile_opt, Q)
+                                                   : std::max(8, std::min(256, Q / 64));
     c->qtiles = ceil_div(Q, c->quartets_per_tile);
     int rc;
     if (prec == MSGPU_PREC_C128) {
@@ -972,15 +981,13 @@ int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
     {
         Timed tm(c, KC_APPLY);
         if (prec == MSGPU_PREC_C128) {
-            if ((e = cudaFuncSetAttribute(k_resident<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(smem))))
+            if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_resident<double2, false>), static_cast<int>(smem))))
                 return cuda_fail(c, e, "resident shared memory");
             k_resident<double2, false><<<blocks, 32 * warps, smem, st>>>(
                 static_cast<const ResidentSystem *>(c->sys_d.p), static_cast<const ResidentWork *>(c->work_d.p), M, wb,
                 static_cast<int *>(c->status.p));
         } else {
-            if ((e = cudaFuncSetAttribute(k_resident<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(smem))))
+            if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_resident<float2, true>), static_cast<int>(smem))))
                 return cuda_fail(c, e, "resident shared memory");
             k_resident<float2, true><<<blocks, 32 * warps, smem, st>>>(
                 static_cast<const ResidentSystem *>(c->sys_d.p), static_cast<const ResidentWork *>(c->work_d.p), M, wb,
@@ -1408,7 +1415,7 @@ cudaError_t fused_prepare(const msgpu_ctx *c, FusedFn fn, int C)
 {
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
-    if (!e) e = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (!e) e = raise_smem_limit(reinterpret_cast<const void *>(fn), optin);
     if (!e && C > 8)
         e = cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     return e;
@@ -1534,12 +1541,12 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
     const int *base = static_cast<const int *>(c->qbase.p);
     if (cb == 4) {
         const int smem = TcCfg<4>::smem(P);
-        cudaFuncSetAttribute(k_lanczos_apply_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<4>), smem);
         k_lanczos_apply_tc<4><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     } else {
         const int smem = TcCfg<3>::smem(P);
-        cudaFuncSetAttribute(k_lanczos_apply_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<3>), smem);
         k_lanczos_apply_tc<3><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     }
@@ -1576,7 +1583,7 @@ void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st,
     size_t smem = 0;
     apply_fits(c, v, qt, &smem);
     grid.y = width / (64 * kApplyVariants[v].np);
-    if (smem) cudaFuncSetAttribute(kApplyVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (smem) raise_smem_limit(reinterpret_cast<const void *>(kApplyVariants[v].fn), static_cast<int>(smem));
     kApplyVariants[v].fn<<<grid, kThreads, smem, st>>>(quartet_view(c), w, s, U, part, c->D / 4, c->s1, c->s2, c->ldm,
                                                        qt);
 }
@@ -1902,8 +1909,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     const double kappa = c->k_scalar ? c->kappa : 0.0;
     const size_t expm_smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
     const int expm_warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / expm_smem_warp)));
-    if ((e = cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(expm_warps * expm_smem_warp))))
+    if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_krylov_expm), static_cast<int>(expm_warps * expm_smem_warp))))
         return cuda_fail(c, e, "expm shared memory");
 
     // Taylor propagator: the shift mu = trace(G)/D and a bound on ||G - mu I||_1
@@ -2393,8 +2399,7 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
     }
     const size_t smem_warp = (4 * static_cast<size_t>(m) * m + m) * sizeof(double2);
     const int warps = std::max(1, std::min(8, static_cast<int>(160 * 1024 / smem_warp)));
-    if (cudaFuncSetAttribute(k_krylov_expm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(warps * smem_warp)) != cudaSuccess)
+    if (raise_smem_limit(reinterpret_cast<const void *>(k_krylov_expm), static_cast<int>(warps * smem_warp)) != cudaSuccess)
         return MSGPU_ERR_CUDA;
     k_krylov_expm<<<ceil_div(ldm, warps), 32 * warps, warps * smem_warp, st>>>(hess, nullptr, nullptr, 0.0, mdim, beta0,
                                                                               nullptr, m, ldm, ntraj, dt, coef, status);

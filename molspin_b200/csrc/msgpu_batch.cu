@@ -189,7 +189,7 @@ int prepare(msgpu_batch *b, int ntimes, int m, int accumulate, long long step_of
 int launch(msgpu_batch *b, int grid, size_t slice, size_t smem, int nlarge, int nitems, int m, bool use_graph)
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem))))
+    if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_batch), static_cast<int>(smem))))
         return bfail(b, MSGPU_ERR_CUDA, std::string("batch: shared memory: ") + cudaGetErrorString(e));
     const size_t key = (static_cast<size_t>(grid) << 40) ^ (slice << 8) ^ (static_cast<size_t>(nlarge) << 20) ^
                        static_cast<size_t>(nitems) ^ (static_cast<size_t>(m) << 56) ^ reinterpret_cast<size_t>(b->scratch.p) ^

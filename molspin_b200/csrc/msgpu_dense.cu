@@ -794,8 +794,8 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     }
     cudaError_t e;
     const int smem = ns == 2 ? GemmCfg<2>::Smem : GemmCfg<3>::Smem;
-    if ((e = cudaFuncSetAttribute(k_dense_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<2>::Smem)) ||
-        (e = cudaFuncSetAttribute(k_dense_gemm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<3>::Smem))) {
+    if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm<2>), GemmCfg<2>::Smem)) ||
+        (e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm<3>), GemmCfg<3>::Smem))) {
         err = std::string("dense: shared memory: ") + cudaGetErrorString(e);
         return MSGPU_ERR_CUDA;
     }

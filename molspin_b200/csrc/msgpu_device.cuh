@@ -10,9 +10,34 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "msgpu_philox.h"
 
 namespace msgpu {
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` and never lowers it.  The limit is one attribute per kernel,
+// shared by every context of the process; contexts driven from several host
+// threads (the batching form's large systems) would otherwise race: a smaller
+// value set by one thread between another thread's set and launch fails that
+// launch with an invalid argument.
+inline cudaError_t raise_smem_limit(const void *fn, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int &cur = limit[{dev, fn}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 // ------------------------------------------------------------ complex helpers
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
