@@ -50,7 +50,7 @@ def _args():
                          "tensor-core propagator; batching: 64 uneven systems; serving: a request stream")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=4.0, help="serving: Poisson arrival rate (requests/s)")
-    ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6")
+    ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6 | int8x4")
     ap.add_argument("--spmm-variant", type=int, default=-1,
                     help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
     ap.add_argument("--combine-tile", type=int, default=0,
@@ -540,12 +540,18 @@ def run_dense(args):
     launches = p.launch_count() - l0[0]
     gms, gn = p.profile_read(6)
     p.profile(False)
-    nprod = 3 if prec == "bf16x3" else 6
+    nprod = {"bf16x3": 3, "bf16x6": 6, "int8x4": 10}[prec]
     Dp = (2 * D + 127) // 128 * 128
     flops = 2.0 * Dp * Dp * M * nprod
     achieved = flops / (gms / gn / 1e3) / 1e12 if gn else None
     peaks = _peaks()
     peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    # int8 products: the dense int8 rate of the tensor cores is twice the BF16
+    # rate; no int8 figure is measured, so the peak is twice the measured BF16
+    peak_note = "measured sustained BF16" if "bf16_tflops_sustained" in peaks else "fallback BF16"
+    if prec == "int8x4":
+        peak *= 2.0
+        peak_note = "twice the " + peak_note + " (int8 rate)"
     # DRAM bytes per GEMM launch from one ncu capture (bf16x3, D=1024, M=4096:
     # 55.1 MB read + 6.8 MB written; the output stays partly in L2)
     traffic = 61.9e6 if (D, M, prec) == (1024, 4096, "bf16x3") else None
@@ -575,13 +581,16 @@ def run_dense(args):
         "metric": "SSE traj-steps/s (dense tensor-core propagator, D=1024)",
         "value": world * M * chunk * args.steps / (el / 1e3), "unit": "traj-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": f"{prec} split BF16, FP32 accumulate",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("int8x4: four int8 slices, exact int32 accumulation, FP64 state" if prec == "int8x4"
+                  else f"{prec} split BF16, FP32 accumulate"),
         "data": "synthetic (seeded)",
         "config": {"workload": w.name, "trajectories_per_gpu": M, "time_steps_per_bench_step": chunk,
                    "renormalize": "exact Haberkorn survival", "l2": "state 2 x 33 MiB + U 16-24 MiB per step"},
-        "roofline": {"bound": "tensor", "kernel": "k_dense_gemm", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak if achieved else None, "traffic": traffic,
-                     "peak_kind": "measured sustained" if "bf16_tflops_sustained" in peaks else "fallback",
+        "roofline": {"bound": "tensor", "kernel": "k_dense_gemm_i8" if prec == "int8x4" else "k_dense_gemm",
+                     "achieved": achieved, "peak": peak,
+                     "unit": "TOP/s" if prec == "int8x4" else "TFLOP/s", "frac": achieved / peak if achieved else None,
+                     "traffic": traffic, "peak_kind": peak_note,
                      "flops_per_launch": flops, "avg_launch_ms": gms / gn if gn else None,
                      "launches_timed": gn, "timing": "CUDA events around every 8th GEMM (sampled)",
                      "share_of_step": (gms / gn) * chunk * args.steps / el if gn and el else None},
@@ -686,6 +695,7 @@ def run_serving(args):
                    "slots": 8, "hbm_budget_gib": 120},
         "latency_s": {"p50": s["p50_latency_s"], "p99": s["p99_latency_s"], "mean": s["mean_latency_s"]},
         "completed": s["completed"], "failed": s["failed"], "max_concurrency": eng.max_concurrency,
+        "contexts": {"created": eng.contexts_created, "reused": eng.contexts_reused},
         "peak_reserved_gib": eng.peak_reserved / 2 ** 30,
         "roofline": {"bound": "hbm", "kernel": "whole stream ((4m+1) D c bytes per traj-step)", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,

@@ -73,6 +73,12 @@ extern "C" {
 #define MSGPU_PROP_RK4 3
 #define MSGPU_PREC_BF16X3 2
 #define MSGPU_PREC_BF16X6 3
+/* Dense propagator with exact accumulation: U and the state are cut into four
+ * int8 slices each (a power-of-two scale per row of U and per trajectory),
+ * the ten slice products up to the fourth level run as tcgen05.mma kind::i8
+ * with int32 accumulators (exact), and the levels are combined in FP64 into
+ * an FP64 state.  No FP32 rounding enters the step. */
+#define MSGPU_PREC_INT8X4 4
 
 /* Options (msgpu_set_option). */
 #define MSGPU_OPT_DENSE_RENORMALIZE 1 /* 1 (default): the dense form restores the exact

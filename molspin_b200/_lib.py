@@ -39,6 +39,7 @@ OPT_TRAJ_GROUPS = 5
 OPT_COMBINE_TILE = 6
 PREC_BF16X3 = 2
 PREC_BF16X6 = 3
+PREC_INT8X4 = 4
 OPT_DENSE_RENORMALIZE = 1
 NOISE_NONE = 0
 NOISE_REPLAY = 1

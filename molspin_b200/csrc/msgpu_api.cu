@@ -838,7 +838,7 @@ int run_dense(msgpu_ctx *c, const msgpu_run_params *p)
     run.renormalize = c->dense_renorm;
     run.status = static_cast<int *>(c->status.p);
     run.part = static_cast<double *>(c->dense_part.p);
-    const int parts = p->precision == MSGPU_PREC_BF16X6 ? 3 : 2;
+    const int parts = p->precision == MSGPU_PREC_INT8X4 ? 4 : p->precision == MSGPU_PREC_BF16X6 ? 3 : 2;
     const double dt = p->ntimes > 1 ? p->times[1] - p->times[0] : 1.0;
     for (int s = 1; s + 1 < p->ntimes; ++s)
         if (std::abs((p->times[s + 1] - p->times[s]) - dt) > 1e-12 * std::abs(dt))
@@ -1278,7 +1278,7 @@ int build_tc(msgpu_ctx *c)
         if (mask[q] != mask[0]) return MSGPU_OK;
     int rc;
     if ((rc = ensure(c, c->tc_src, sizeof(int2) * nent, "tensor-core SpMM table entries")) ||
-        (rc = ensure(c, c->tc_tab, static_cast<size_t>(nent) * 3 * kTcB, "tensor-core SpMM tables")))
+        (rc = ensure(c, c->tc_tab, static_cast<size_t>(nent) * 2 * kTcB, "tensor-core SpMM tables")))
         return rc;
     cudaError_t e;
     if ((e = cudaMemcpyAsync(c->tc_src.p, src.data(), sizeof(int2) * nent, cudaMemcpyHostToDevice, c->stream)) ||
@@ -1535,7 +1535,7 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
 {
     const int Q = c->D / 4, P = c->tc_P;
     const unsigned char *tflip = static_cast<const unsigned char *>(c->tc_tab.p);
-    const unsigned char *tdiag = tflip + static_cast<size_t>(2 * P) * 3 * kTcB;
+    const unsigned char *tdiag = tflip + static_cast<size_t>(2 * P) * 2 * kTcB;
     const dim3 grid(Q >> cb, ceil_div(width, kTcTraj));
     int *status = static_cast<int *>(c->status.p);
     const int *base = static_cast<const int *>(c->qbase.p);
@@ -1777,8 +1777,10 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         return fail(c, MSGPU_ERR_INVALID, "run: the Hamiltonian schedule does not cover the requested steps");
     if (p->propagator == MSGPU_PROP_DENSE) {
         if (c->sched_steps) return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator needs a time-independent H");
-        if (p->precision != MSGPU_PREC_BF16X3 && p->precision != MSGPU_PREC_BF16X6)
-            return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator takes MSGPU_PREC_BF16X3 or MSGPU_PREC_BF16X6");
+        if (p->precision != MSGPU_PREC_BF16X3 && p->precision != MSGPU_PREC_BF16X6 &&
+            p->precision != MSGPU_PREC_INT8X4)
+            return fail(c, MSGPU_ERR_INVALID,
+                        "run: the dense propagator takes MSGPU_PREC_BF16X3, MSGPU_PREC_BF16X6 or MSGPU_PREC_INT8X4");
         if (c->D > 4096) return fail(c, MSGPU_ERR_INVALID, "run: the dense propagator is limited to dimension 4096");
         if (c->noise_mode == MSGPU_NOISE_REPLAY &&
             (c->bits_ntraj != c->M || p->step_offset < 0 || p->step_offset + (p->ntimes - 1) > c->bits_steps))

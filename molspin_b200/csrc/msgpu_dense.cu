@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "msgpu.h"
@@ -293,6 +294,183 @@ k_dense_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CU
     }
 }
 
+// ------------------------------------------------------------ int8 form
+// Exact-accumulation GEMM.  Each operand is x = 2^e sum_{i<4} a_i / (127 254^i)
+// with int8 slices a_i (a per-row scale for U, a per-trajectory scale for the
+// state).  The products a_i b_j with i + j = L share the weight
+// 1 / (127^2 254^L), so they are summed in one int32 accumulator per level L
+// (exactly: |a_i b_j| <= 127^2 and at most 4 K-long products per level stay
+// below 2^31 for K <= 8192), and the epilogue combines the four levels in FP64
+// with the two scales.  The FP32 rounding of the BF16 forms is gone: the only
+// errors are the slices' truncation (2^-31 of the scale) and the FP64 state.
+constexpr int kIK = 64;              // K (int8) per stage: one 64-byte swizzle row
+constexpr int kIStages = 3;
+constexpr int kIBN = 128;            // trajectories per CTA
+constexpr int kIParts = 4;           // slices per operand
+constexpr int kIATile = kGM * kIK;   // bytes of one A slice tile (8 KB)
+constexpr int kIBTile = kIBN * kIK;  // bytes of one B slice tile (8 KB)
+constexpr int kIStage = kIParts * (kIATile + kIBTile);
+constexpr int kISmem = kIStages * kIStage + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int kILevels = 4;          // TMEM: 4 x 128 = 512 columns
+
+// UMMA shared-memory descriptor: K-major operand, 64-byte swizzle, rows of 64
+// bytes in 8-row (512-byte) groups: SBO = 512 B, LBO unused (1), version 1,
+// layout type SWIZZLE_64B (4).
+__device__ __forceinline__ uint64_t umma_desc64(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>(512 >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= static_cast<uint64_t>(4) << 61;
+    return d;
+}
+
+// kind::i8 instruction descriptor: D = S32, A = B = signed int8, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_i8(int M, int N)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+           (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// out[n][m] = sum over levels of the exact slice products, scaled:
+//   A slices: Dp x Dp int8 (row-major, K contiguous) -> tensor maps ta[0..4)
+//   B slices: Mp x Dp int8                          -> tensor maps tb[0..4)
+//   sa[m], sb[n]: the power-of-two scales of U's row m and trajectory n
+// grid = (trajectory tiles of this launch, Dp / 128), block = 128 threads.
+__global__ void __launch_bounds__(kGThreads, 1)
+k_dense_gemm_i8(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
+                const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap ta3,
+                const __grid_constant__ CUtensorMap tb0, const __grid_constant__ CUtensorMap tb1,
+                const __grid_constant__ CUtensorMap tb2, const __grid_constant__ CUtensorMap tb3,
+                const double *__restrict__ sa, const double *__restrict__ sb, double *__restrict__ out, int Dp,
+                int n_tile0, int *__restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char *base_ptr = smem_raw + (base - raw);
+    const uint32_t bars = base + kIStages * kIStage;  // full[3], empty[3], accum
+    uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(base_ptr + kIStages * kIStage);
+    volatile int *abort = reinterpret_cast<volatile int *>(bar_ptr + 8);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ptr + 9);
+    const uint32_t full0 = bars, empty0 = bars + 8 * kIStages, accum = bars + 16 * kIStages;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = (n_tile0 + blockIdx.x) * kIBN, m0 = blockIdx.y * kGM;
+    const int nk = Dp / kIK;
+    const CUtensorMap *ta[4] = {&ta0, &ta1, &ta2, &ta3};
+    const CUtensorMap *tb[4] = {&tb0, &tb1, &tb2, &tb3};
+
+    if (threadIdx.x == 0) {
+        *abort = 0;
+        for (int s = 0; s < kIStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * s));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * s));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(accum));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kILevels * kIBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kIStages, r = kb / kIStages;
+            if (!mbar_wait(empty0 + 8 * s, (r & 1) ^ 1, abort)) break;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * s), "r"(kIStage));
+            const uint32_t st = base + s * kIStage;
+            for (int p = 0; p < kIParts; ++p) tma_load_2d(st + p * kIATile, ta[p], kb * kIK, m0, full0 + 8 * s);
+            for (int q = 0; q < kIParts; ++q)
+                tma_load_2d(st + kIParts * kIATile + q * kIBTile, tb[q], kb * kIK, n0, full0 + 8 * s);
+            issued = kb + 1;
+        }
+        for (int kb = max(0, issued - kIStages); kb < issued; ++kb) {
+            const int s = kb % kIStages, r = kb / kIStages;
+            for (uint32_t it = 0; it < kWaitLimit && !mbar_try(full0 + 8 * s, r & 1); ++it) {
+            }
+        }
+    } else if (threadIdx.x == 32) {
+        // MMA issuer: level L = i + j accumulates a_i b_j
+        constexpr uint32_t idesc = umma_idesc_i8(kGM, kIBN);
+        uint32_t on = 0;  // bit L: level L's accumulator was written
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % kIStages, r = kb / kIStages;
+            if (!mbar_wait(full0 + 8 * s, r & 1, abort)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * kIStage;
+#pragma unroll
+            for (int kk = 0; kk < kIK / 32; ++kk)
+#pragma unroll
+                for (int i = 0; i < kIParts; ++i)
+#pragma unroll
+                    for (int j = 0; j < kIParts - i; ++j) {
+                        const int L = i + j;
+                        const uint64_t ad = umma_desc64(st + i * kIATile + kk * 32);
+                        const uint64_t bd = umma_desc64(st + kIParts * kIATile + j * kIBTile + kk * 32);
+                        umma_i8(tmem + L * kIBN, ad, bd, idesc, (on >> L) & 1u);
+                        on |= 1u << L;
+                    }
+            umma_commit(empty0 + 8 * s);
+        }
+        umma_commit(accum);
+    }
+    __syncwarp();
+
+    bool ok = mbar_wait(accum, 0, abort);
+    if (!ok) {
+        for (uint32_t it = 0; it < kWaitLimit && !mbar_try(accum, 0); ++it) {
+        }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && !*abort) {
+        const int row = m0 + 32 * warp + lane;
+        const double s_row = sa[row];
+        const uint32_t lane_base = tmem + (static_cast<uint32_t>(32 * warp) << 16);
+        constexpr double w0 = 1.0 / (127.0 * 127.0), w1 = w0 / 254.0, w2 = w1 / 254.0, w3 = w2 / 254.0;
+#pragma unroll 1
+        for (int c = 0; c < kIBN; c += 16) {
+            uint32_t v[kILevels][16];
+#pragma unroll
+            for (int L = 0; L < kILevels; ++L) tmem_ld16_issue(lane_base + static_cast<uint32_t>(L * kIBN + c), v[L]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const double y = static_cast<double>(static_cast<int>(v[3][j])) * w3 +
+                                 static_cast<double>(static_cast<int>(v[2][j])) * w2 +
+                                 static_cast<double>(static_cast<int>(v[1][j])) * w1 +
+                                 static_cast<double>(static_cast<int>(v[0][j])) * w0;
+                out[static_cast<size_t>(n0 + c + j) * Dp + row] = y * s_row * sb[n0 + c + j];
+            }
+        }
+    }
+    if (*abort && threadIdx.x == 0) atomicOr(status, 4);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kILevels * kIBN));
+    }
+}
+
 // ------------------------------------------------------------ U precompute
 // C = scale * (A B) + (add_identity ? I : 0); n x n complex row-major.
 __global__ void k_zgemm(const double2 *__restrict__ A, const double2 *__restrict__ B, double2 *__restrict__ C, int n,
@@ -378,22 +556,62 @@ __global__ void k_u_split(const double2 *__restrict__ U, int n, int Dp, int ns, 
     for (int k = 0; k < ns; ++k) parts[static_cast<size_t>(k) * Dp * Dp + idx] = p[k];
 }
 
-// context state (ldm x D interleaved complex128) <-> dense state (Mp x Dp fp32)
-__global__ void k_ctx_to_dense(const double2 *__restrict__ psi, int D, int M, int ldm, int Dp, int Mp,
-                               float *__restrict__ out)
+// U (n x n complex) -> real interleaved Dp x Dp matrix, row r scaled by its
+// power of two 2^e_r >= max_c |A[r][c]| and cut into four int8 slices (the
+// operand form of k_dense_gemm_i8: r = A / 2^e, a_0 = rint(127 r), then
+// a_i = rint(254 r_i) on the remainders); one block of 256 threads per row.
+__global__ void __launch_bounds__(256) k_u_split_i8(const double2 *__restrict__ U, int n, int Dp,
+                                                    int8_t *__restrict__ parts, double *__restrict__ scale)
+{
+    __shared__ double red[8];
+    const int i = blockIdx.x;
+    auto val = [&](int j) -> double {
+        if (i >= 2 * n || j >= 2 * n) return 0.0;
+        const double2 u = U[static_cast<size_t>(i >> 1) * n + (j >> 1)];
+        const int c = i & 1, d = j & 1;
+        return (c == d) ? u.x : (c == 0 ? -u.y : u.y);
+    };
+    double m = 0.0;
+    for (int j = threadIdx.x; j < Dp; j += blockDim.x) m = fmax(m, fabs(val(j)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    const double s = m > 0.0 ? exp2(ceil(log2(m))) : 1.0, inv = 1.0 / s;
+    if (threadIdx.x == 0) scale[i] = s;
+    for (int j = threadIdx.x; j < Dp; j += blockDim.x) {
+        double r = val(j) * inv;
+        double q = rint(127.0 * r);
+        parts[static_cast<size_t>(i) * Dp + j] = static_cast<int8_t>(q);
+        r = 127.0 * r - q;
+        for (int p = 1; p < 4; ++p) {
+            q = rint(254.0 * r);
+            parts[(static_cast<size_t>(p) * Dp + i) * Dp + j] = static_cast<int8_t>(q);
+            r = 254.0 * r - q;
+        }
+    }
+}
+
+// context state (ldm x D interleaved complex128) <-> dense state (Mp x Dp, T = fp32 or fp64)
+template <typename T>
+__global__ void k_ctx_to_dense_t(const double2 *__restrict__ psi, int D, int M, int ldm, int Dp, int Mp,
+                                 T *__restrict__ out)
 {
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= static_cast<size_t>(Mp) * Dp) return;
     const int t = static_cast<int>(idx / Dp), k = static_cast<int>(idx % Dp);
-    float v = 0.f;
+    T v = 0;
     if (t < M && k < 2 * D) {
         const double2 z = psi[static_cast<size_t>(k >> 1) * ldm + t];
-        v = static_cast<float>((k & 1) ? z.y : z.x);
+        v = static_cast<T>((k & 1) ? z.y : z.x);
     }
     out[idx] = v;
 }
 
-__global__ void k_dense_to_ctx(const float *__restrict__ in, int D, int M, int ldm, int Dp, double2 *__restrict__ psi)
+template <typename T>
+__global__ void k_dense_to_ctx_t(const T *__restrict__ in, int D, int M, int ldm, int Dp, double2 *__restrict__ psi)
 {
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= static_cast<size_t>(D) * ldm) return;
@@ -467,27 +685,37 @@ __device__ __forceinline__ double dense_ensemble_sum(const double *__restrict__ 
     return v;
 }
 
-// One CTA (256 threads) per trajectory.  The trajectory's column (2D floats,
+// One CTA (128 threads) per trajectory.  The trajectory's column (2D values,
 // re/im per row) is staged in shared memory once; flips, the norm, the
-// optional renormalisation, the pair observables and the BF16 split of the
-// next GEMM operand all work from there, and the FP32 column is written back
-// only at the last time point (the next GEMM overwrites it otherwise).
-// Blocks 0..nobs-1 also sum the previous time point's per-trajectory values
-// into its ensemble values, which saves a launch per step.
+// optional renormalisation, the pair observables and the split of the next
+// GEMM operand all work from there, and the column is written back only at
+// the last time point (the next GEMM overwrites it otherwise).  Blocks
+// 0..nobs-1 also sum the previous time point's per-trajectory values into its
+// ensemble values, which saves a launch per step.
+//   kI8 = false: FP32 state, BF16 parts (E.ns of them) for k_dense_gemm.
+//   kI8 = true:  FP64 state, four int8 slices and the column's power-of-two
+//                scale for k_dense_gemm_i8 (see k_u_split_i8 for the slicing).
 constexpr int kEpiThreads = 128;
-__global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__restrict__ psi,
-                                                                __nv_bfloat16 *__restrict__ bparts, DenseEpi E)
+template <bool kI8>
+__global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(void *__restrict__ psi_v, void *__restrict__ bparts_v,
+                                                                double *__restrict__ bscale, DenseEpi E)
 {
-    extern __shared__ float4 s_col4[];  // D/2 float4 = the 2D floats of the column
-    float2 *s_col = reinterpret_cast<float2 *>(s_col4);
-    __shared__ double red[9][8];
-    __shared__ double s_scale;
+    using V2 = typename std::conditional<kI8, double2, float2>::type;
+    extern __shared__ float4 s_col4[];  // the 2D values of the column
+    V2 *s_col = reinterpret_cast<V2 *>(s_col4);
+    __shared__ double red[10][8];
+    __shared__ double s_scale, s_max;
     __shared__ double2 s_obs[8][10];
     const int t = E.t0 + blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *col = psi + static_cast<size_t>(t) * E.Dp;
     if (threadIdx.x < 80) s_obs[threadIdx.x / 10][threadIdx.x % 10] = E.obs_c[threadIdx.x / 10][threadIdx.x % 10];
-    const int n4 = E.D / 2;
-    for (int i = threadIdx.x; i < n4; i += kEpiThreads) s_col4[i] = reinterpret_cast<const float4 *>(col)[i];
+    if constexpr (kI8) {
+        const double2 *col = static_cast<const double2 *>(psi_v) + static_cast<size_t>(t) * (E.Dp / 2);
+        for (int i = threadIdx.x; i < E.D; i += kEpiThreads) s_col[i] = col[i];
+    } else {
+        const float *col = static_cast<const float *>(psi_v) + static_cast<size_t>(t) * E.Dp;
+        const int n4 = E.D / 2;
+        for (int i = threadIdx.x; i < n4; i += kEpiThreads) s_col4[i] = reinterpret_cast<const float4 *>(col)[i];
+    }
     const int Q = E.D / 4;
     int flip = 0;
     if (t < E.M) {
@@ -508,29 +736,33 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
     const double ref = (threadIdx.x == 0 && t < E.M && !E.init) ? E.norm0[t] : 0.0;
     __syncthreads();
     // one pass over the quartets (each belongs to one thread): flip in shared
-    // memory, norm and pair observables of the unscaled state.  Observables
-    // are quadratic, so the renormalisation enters as sc^2 afterwards.
-    double nn = 0.0;
+    // memory, norm and pair observables of the unscaled state, and (int8
+    // operands) the largest component.  Observables are quadratic, so the
+    // renormalisation enters as sc^2 afterwards.
+    double nn = 0.0, mx = 0.0;
     double obs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1
     for (int q = threadIdx.x; q < Q; q += kEpiThreads) {
         const int b = quartet_base(q, E.s1, E.s2);
         const int r[4] = {b, b + E.s2, b + E.s1, b + E.s1 + E.s2};
-        float2 x[4];
+        V2 x[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) x[a] = s_col[r[a]];
         if (flip) {
-            const float2 c1 = x[1];
-            x[0] = make_float2(-x[0].x, -x[0].y);
-            x[1] = make_float2(-x[2].x, -x[2].y);
-            x[2] = make_float2(-c1.x, -c1.y);
-            x[3] = make_float2(-x[3].x, -x[3].y);
+            const V2 c1 = x[1];
+            x[0].x = -x[0].x; x[0].y = -x[0].y;
+            x[1].x = -x[2].x; x[1].y = -x[2].y;
+            x[2].x = -c1.x;   x[2].y = -c1.y;
+            x[3].x = -x[3].x; x[3].y = -x[3].y;
 #pragma unroll
             for (int a = 0; a < 4; ++a) s_col[r[a]] = x[a];
         }
         double2 v[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) v[a] = make_double2(x[a].x, x[a].y);
+        if (kI8)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) mx = fmax(mx, fmax(fabs(v[a].x), fabs(v[a].y)));
         nn += v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y + v[2].x * v[2].x +
               v[2].y * v[2].y + v[3].x * v[3].x + v[3].y * v[3].y;
         const volatile double2 *so = &s_obs[0][0];  // re-read per use: nothing is held in registers
@@ -553,6 +785,11 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
     }
     nn = warp_sum(nn);
     if (lane == 0) red[8][warp] = nn;
+    if (kI8) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) red[9][warp] = mx;
+    }
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
         if (o >= E.nobs) break;
@@ -561,8 +798,11 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double cur = 0.0;
-        for (int w = 0; w < kEpiThreads / 32; ++w) cur += red[8][w];
+        double cur = 0.0, m = 0.0;
+        for (int w = 0; w < kEpiThreads / 32; ++w) {
+            cur += red[8][w];
+            if (kI8) m = fmax(m, red[9][w]);
+        }
         double sc = 1.0;
         if (E.init) {
             if (t < E.M) E.norm0[t] = cur;
@@ -570,43 +810,84 @@ __global__ void __launch_bounds__(kEpiThreads, 8) k_dense_epilogue(float *__rest
             sc = sqrt(ref * exp(-E.decay * E.elapsed) / cur);
         }
         s_scale = sc;
+        s_max = m * sc;
     }
     __syncthreads();
     const double scd = s_scale;
-    const float sc = static_cast<float>(scd);
-    // BF16 split of the scaled state for the next GEMM: 8 floats (two float4)
-    // per thread and part, 16-byte stores, the padding beyond 2D floats zero.
-    // In FP32 each residual x - bf16(x) is exact, so hi + mid + lo carries all
-    // 24 bits of x; conversions are round-to-nearest, two values at a time.
-    const int nc = E.Dp / 8, live = E.D / 4;  // chunks of 8 floats; 2D / 8 of them hold data
-    float4 *col4 = reinterpret_cast<float4 *>(col);
-    for (int c = threadIdx.x; c < nc; c += kEpiThreads) {
-        float f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (c < live) {
-            float4 u = s_col4[2 * c], w = s_col4[2 * c + 1];
-            if (sc != 1.f) {
-                u = make_float4(u.x * sc, u.y * sc, u.z * sc, u.w * sc);
-                w = make_float4(w.x * sc, w.y * sc, w.z * sc, w.w * sc);
+    const int nc = E.Dp / 8, live = E.D / 4;  // chunks of 8 values; 2D / 8 of them hold data
+    if constexpr (kI8) {
+        // int8 slices of the scaled state for the next GEMM.  With the column's
+        // scale 2^e >= max |x|, r = x / 2^e lies in [-1, 1]; a_0 = rint(127 r),
+        // then a_i = rint(254 r_i) on the remainders r_{i+1} = 254 r_i - a_i
+        // (|r_i| <= 1/2), so x = 2^e sum_i a_i / (127 254^i) to 2^-31 of 2^e.
+        const double m = s_max;
+        const double s = m > 0.0 ? exp2(ceil(log2(m))) : 1.0;
+        if (threadIdx.x == 0) bscale[t] = s;
+        const double inv = 1.0 / s;  // a power of two: exact
+        double *colw = static_cast<double *>(psi_v) + static_cast<size_t>(t) * E.Dp;
+        int8_t *bp = static_cast<int8_t *>(bparts_v);
+        for (int c = threadIdx.x; c < nc; c += kEpiThreads) {
+            __align__(8) int8_t a[4][8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                double x = 0.0;
+                if (c < live) {
+                    const double2 z = s_col[4 * c + (j >> 1)];
+                    x = ((j & 1) ? z.y : z.x) * scd;
+                    if (E.store_state) colw[8 * c + j] = x;
+                }
+                double r = x * inv;
+                double q = rint(127.0 * r);
+                a[0][j] = static_cast<int8_t>(q);
+                r = 127.0 * r - q;
+#pragma unroll
+                for (int i = 1; i < 4; ++i) {
+                    q = rint(254.0 * r);
+                    a[i][j] = static_cast<int8_t>(q);
+                    r = 254.0 * r - q;
+                }
             }
-            if (E.store_state) {
-                col4[2 * c] = u;
-                col4[2 * c + 1] = w;
-            }
-            f[0] = u.x; f[1] = u.y; f[2] = u.z; f[3] = u.w;
-            f[4] = w.x; f[5] = w.y; f[6] = w.z; f[7] = w.w;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                *reinterpret_cast<uint2 *>(bp + (static_cast<size_t>(i) * E.Mp + t) * E.Dp + 8 * c) =
+                    *reinterpret_cast<const uint2 *>(a[i]);
         }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            if (i >= E.ns) break;
-            __align__(16) __nv_bfloat162 h[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                h[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
-                f[2 * j] -= __low2float(h[j]);
-                f[2 * j + 1] -= __high2float(h[j]);
+    } else {
+        const float sc = static_cast<float>(scd);
+        // BF16 split of the scaled state for the next GEMM: 8 floats (two float4)
+        // per thread and part, 16-byte stores, the padding beyond 2D floats zero.
+        // In FP32 each residual x - bf16(x) is exact, so hi + mid + lo carries all
+        // 24 bits of x; conversions are round-to-nearest, two values at a time.
+        float4 *col4 = reinterpret_cast<float4 *>(static_cast<float *>(psi_v) + static_cast<size_t>(t) * E.Dp);
+        __nv_bfloat16 *bparts = static_cast<__nv_bfloat16 *>(bparts_v);
+        for (int c = threadIdx.x; c < nc; c += kEpiThreads) {
+            float f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (c < live) {
+                float4 u = s_col4[2 * c], w = s_col4[2 * c + 1];
+                if (sc != 1.f) {
+                    u = make_float4(u.x * sc, u.y * sc, u.z * sc, u.w * sc);
+                    w = make_float4(w.x * sc, w.y * sc, w.z * sc, w.w * sc);
+                }
+                if (E.store_state) {
+                    col4[2 * c] = u;
+                    col4[2 * c + 1] = w;
+                }
+                f[0] = u.x; f[1] = u.y; f[2] = u.z; f[3] = u.w;
+                f[4] = w.x; f[5] = w.y; f[6] = w.z; f[7] = w.w;
             }
-            *reinterpret_cast<uint4 *>(bparts + (static_cast<size_t>(i) * E.Mp + t) * E.Dp + 8 * c) =
-                *reinterpret_cast<const uint4 *>(h);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (i >= E.ns) break;
+                __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    h[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                    f[2 * j] -= __low2float(h[j]);
+                    f[2 * j + 1] -= __high2float(h[j]);
+                }
+                *reinterpret_cast<uint4 *>(bparts + (static_cast<size_t>(i) * E.Mp + t) * E.Dp + 8 * c) =
+                    *reinterpret_cast<const uint4 *>(h);
+            }
         }
     }
     // trapezoid (compensated) and this time point's value, one thread per observable
@@ -683,6 +964,21 @@ bool make_map(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows)
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2D int8 tensor map over a rows x cols row-major matrix, box = 64 x box_rows,
+// 64-byte swizzle (the operand tiles of k_dense_gemm_i8).
+bool make_map_i8(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows)
+{
+    EncodeTiled enc = encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kIK), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 inline int cdiv(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 
 }  // namespace
@@ -691,17 +987,28 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
                   const void *psi128, cudaStream_t stream, std::string &err,
                   int (*alloc)(void *ctx, void **p, size_t bytes, const char *what), void *actx)
 {
-    if (parts != 2 && parts != 3) { err = "dense: split depth must be 2 or 3"; return MSGPU_ERR_INVALID; }
-    const int BN = parts == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
+    if (parts != 2 && parts != 3 && parts != kIParts) {
+        err = "dense: split depth must be 2 or 3 (BF16) or 4 (int8)";
+        return MSGPU_ERR_INVALID;
+    }
+    const bool i8 = parts == kIParts;
+    const int BN = i8 ? kIBN : parts == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
     const int Dp = (2 * D + kGM - 1) / kGM * kGM;
     const int Mp = (M + BN - 1) / BN * BN;
     const bool realloc = st.D != D || st.M != M || st.parts != parts || !st.psi;
     if (realloc) {
         st = DenseState();
         int rc;
-        if ((rc = alloc(actx, &st.u_parts, sizeof(__nv_bfloat16) * parts * static_cast<size_t>(Dp) * Dp, "dense U")) ||
-            (rc = alloc(actx, &st.psi, sizeof(float) * static_cast<size_t>(Mp) * Dp, "dense state")) ||
-            (rc = alloc(actx, &st.b_parts, sizeof(__nv_bfloat16) * parts * static_cast<size_t>(Mp) * Dp, "dense split state")) ||
+        // int8: four byte slices plus the power-of-two scales (rows of U,
+        // trajectories of the state) after them; FP64 state.  BF16: parts
+        // of two bytes; FP32 state.
+        const size_t esz = i8 ? 1 : sizeof(__nv_bfloat16);
+        const size_t u_bytes = esz * parts * static_cast<size_t>(Dp) * Dp + (i8 ? sizeof(double) * Dp : 0);
+        const size_t b_bytes = esz * parts * static_cast<size_t>(Mp) * Dp + (i8 ? sizeof(double) * Mp : 0);
+        if ((rc = alloc(actx, &st.u_parts, u_bytes, "dense U")) ||
+            (rc = alloc(actx, &st.psi, (i8 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(Mp) * Dp,
+                        "dense state")) ||
+            (rc = alloc(actx, &st.b_parts, b_bytes, "dense split state")) ||
             // G, T, W (+ slack) for U; row norms (8D doubles); per-trajectory
             // values (8 Mp doubles) and reference norms (Mp doubles)
             (rc = alloc(actx, &st.work,
@@ -714,6 +1021,8 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
         st.M = M;
         st.Mp = Mp;
         st.parts = parts;
+        st.u_scale = i8 ? static_cast<unsigned char *>(st.u_parts) + static_cast<size_t>(parts) * Dp * Dp : nullptr;
+        st.b_scale = i8 ? static_cast<unsigned char *>(st.b_parts) + static_cast<size_t>(parts) * Mp * Dp : nullptr;
         st.have_u = false;
     }
     cudaError_t e;
@@ -753,7 +1062,11 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
             std::swap(T, W);
         }
         const size_t nu = static_cast<size_t>(Dp) * Dp;
-        k_u_split<<<cdiv(nu, 256), 256, 0, stream>>>(T, D, Dp, parts, static_cast<__nv_bfloat16 *>(st.u_parts));
+        if (i8)
+            k_u_split_i8<<<Dp, 256, 0, stream>>>(T, D, Dp, static_cast<int8_t *>(st.u_parts),
+                                                 static_cast<double *>(st.u_scale));
+        else
+            k_u_split<<<cdiv(nu, 256), 256, 0, stream>>>(T, D, Dp, parts, static_cast<__nv_bfloat16 *>(st.u_parts));
         if ((e = cudaGetLastError())) {
             err = std::string("dense: propagator: ") + cudaGetErrorString(e);
             return MSGPU_ERR_CUDA;
@@ -762,8 +1075,12 @@ int dense_prepare(DenseState &st, int D, int M, int ldm, int parts, double dt, c
         st.dt = dt;
     }
     const size_t ns = static_cast<size_t>(Mp) * Dp;
-    k_ctx_to_dense<<<cdiv(ns, 256), 256, 0, stream>>>(static_cast<const double2 *>(psi128), D, M, ldm, Dp, Mp,
-                                                       static_cast<float *>(st.psi));
+    if (i8)
+        k_ctx_to_dense_t<double><<<cdiv(ns, 256), 256, 0, stream>>>(static_cast<const double2 *>(psi128), D, M, ldm,
+                                                                     Dp, Mp, static_cast<double *>(st.psi));
+    else
+        k_ctx_to_dense_t<float><<<cdiv(ns, 256), 256, 0, stream>>>(static_cast<const double2 *>(psi128), D, M, ldm, Dp,
+                                                                    Mp, static_cast<float *>(st.psi));
     if ((e = cudaGetLastError())) {
         err = std::string("dense: state: ") + cudaGetErrorString(e);
         return MSGPU_ERR_CUDA;
@@ -775,27 +1092,41 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
               float *gemm_ms, long long *gemm_launches, int gemm_every)
 {
     const int D = st.D, Dp = st.Dp, M = st.M, Mp = st.Mp, ns = st.parts;
-    CUtensorMap ta[3], tb[3];
+    const bool i8 = ns == kIParts;
+    CUtensorMap ta[4], tb[4];
     std::memset(ta, 0, sizeof(ta));
     std::memset(tb, 0, sizeof(tb));
-    const int BN = ns == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
-    const __nv_bfloat16 *up = static_cast<const __nv_bfloat16 *>(st.u_parts);
-    __nv_bfloat16 *bp = static_cast<__nv_bfloat16 *>(st.b_parts);
+    const int BN = i8 ? kIBN : ns == 2 ? GemmCfg<2>::BN : GemmCfg<3>::BN;
+    void *bp = st.b_parts;
     for (int p = 0; p < ns; ++p) {
-        if (!make_map(&ta[p], up + static_cast<size_t>(p) * Dp * Dp, Dp, Dp, kGM) ||
-            !make_map(&tb[p], bp + static_cast<size_t>(p) * Mp * Dp, Mp, Dp, BN)) {
+        bool okm;
+        if (i8)
+            okm = make_map_i8(&ta[p], static_cast<const int8_t *>(st.u_parts) + static_cast<size_t>(p) * Dp * Dp, Dp, Dp,
+                              kGM) &&
+                  make_map_i8(&tb[p], static_cast<const int8_t *>(st.b_parts) + static_cast<size_t>(p) * Mp * Dp, Mp, Dp,
+                              BN);
+        else
+            okm = make_map(&ta[p], static_cast<const __nv_bfloat16 *>(st.u_parts) + static_cast<size_t>(p) * Dp * Dp, Dp,
+                           Dp, kGM) &&
+                  make_map(&tb[p], static_cast<const __nv_bfloat16 *>(st.b_parts) + static_cast<size_t>(p) * Mp * Dp, Mp,
+                           Dp, BN);
+        if (!okm) {
             err = "dense: cannot encode TMA tensor maps (cuTensorMapEncodeTiled unavailable or rejected)";
             return MSGPU_ERR_CUDA;
         }
     }
-    for (int p = ns; p < 3; ++p) {
+    for (int p = ns; p < 4; ++p) {
         ta[p] = ta[0];
         tb[p] = tb[0];
     }
     cudaError_t e;
-    const int smem = ns == 2 ? GemmCfg<2>::Smem : GemmCfg<3>::Smem;
+    const int smem = i8 ? kISmem : ns == 2 ? GemmCfg<2>::Smem : GemmCfg<3>::Smem;
+    const size_t epi_smem = (i8 ? sizeof(double) : sizeof(float)) * 2 * static_cast<size_t>(D);
     if ((e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm<2>), GemmCfg<2>::Smem)) ||
-        (e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm<3>), GemmCfg<3>::Smem))) {
+        (e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm<3>), GemmCfg<3>::Smem)) ||
+        (e = raise_smem_limit(reinterpret_cast<const void *>(k_dense_gemm_i8), kISmem)) ||
+        (e = raise_smem_limit(reinterpret_cast<const void *>(i8 ? k_dense_epilogue<true> : k_dense_epilogue<false>),
+                              static_cast<int>(epi_smem)))) {
         err = std::string("dense: shared memory: ") + cudaGetErrorString(e);
         return MSGPU_ERR_CUDA;
     }
@@ -804,7 +1135,6 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     // (8 observables at most each), then the renormalisation references
     double *tv[2] = {tvals, tvals + 8 * static_cast<size_t>(Mp)};
     double *norm0 = tvals + 16 * static_cast<size_t>(Mp);
-    const size_t epi_smem = sizeof(float) * 2 * static_cast<size_t>(D);
     DenseEpi E;
     std::memset(&E, 0, sizeof(E));
     E.D = D;
@@ -876,11 +1206,20 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
         Eg.t0 = gt[g] * BN;
         Eg.t1 = gt[g + 1] * BN;
         Eg.prev_values = point_prev >= 0 ? run.part + g * nv + static_cast<size_t>(point_prev) * run.nobs : nullptr;
-        k_dense_epilogue<<<Eg.t1 - Eg.t0, kEpiThreads, epi_smem, ss[g]>>>(static_cast<float *>(st.psi), bp, Eg);
+        if (i8)
+            k_dense_epilogue<true><<<Eg.t1 - Eg.t0, kEpiThreads, epi_smem, ss[g]>>>(
+                st.psi, bp, static_cast<double *>(st.b_scale), Eg);
+        else
+            k_dense_epilogue<false><<<Eg.t1 - Eg.t0, kEpiThreads, epi_smem, ss[g]>>>(st.psi, bp, nullptr, Eg);
     };
     auto gemm = [&](int g, cudaStream_t sg) {
         dim3 grid(gt[g + 1] - gt[g], Dp / kGM);
-        if (ns == 2)
+        if (i8)
+            k_dense_gemm_i8<<<grid, kGThreads, smem, sg>>>(ta[0], ta[1], ta[2], ta[3], tb[0], tb[1], tb[2], tb[3],
+                                                           static_cast<const double *>(st.u_scale),
+                                                           static_cast<const double *>(st.b_scale),
+                                                           static_cast<double *>(st.psi), Dp, gt[g], run.status);
+        else if (ns == 2)
             k_dense_gemm<2><<<grid, kGThreads, smem, sg>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2],
                                                            static_cast<float *>(st.psi), Dp, gt[g], run.status);
         else
@@ -960,8 +1299,12 @@ int dense_run(DenseState &st, const DenseRun &run, void *psi128, int ldm, cudaSt
     for (auto &ev : evs) cudaEventDestroy(ev);
     if (gemm_launches) *gemm_launches = gemm_ms ? ntimed : steps;  // full-block GEMMs the time covers
     const size_t nc = static_cast<size_t>(D) * ldm;
-    k_dense_to_ctx<<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const float *>(st.psi), D, M, ldm, Dp,
-                                                       static_cast<double2 *>(psi128));
+    if (i8)
+        k_dense_to_ctx_t<double><<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const double *>(st.psi), D, M, ldm, Dp,
+                                                                     static_cast<double2 *>(psi128));
+    else
+        k_dense_to_ctx_t<float><<<cdiv(nc, 256), 256, 0, stream>>>(static_cast<const float *>(st.psi), D, M, ldm, Dp,
+                                                                    static_cast<double2 *>(psi128));
     if ((e = cudaGetLastError())) {
         err = std::string("dense: state: ") + cudaGetErrorString(e);
         return MSGPU_ERR_CUDA;

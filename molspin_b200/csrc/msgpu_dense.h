@@ -13,12 +13,14 @@ namespace msgpu {
 struct DenseState {
     int D = 0, Dp = 0;        // dimension, padded real-interleaved size 2D rounded up to 128
     int M = 0, Mp = 0;        // trajectories, padded to the GEMM N tile
-    int parts = 0;            // BF16 split depth (2 or 3)
+    int parts = 0;            // BF16 split depth (2 or 3), or 4: int8 slices (exact accumulation)
     double dt = 0.0;          // step U was built for
     bool have_u = false;
     void *u_parts = nullptr;  // parts x Dp x Dp bf16 (real interleaved U, K-major rows)
-    void *psi = nullptr;      // Mp x Dp fp32, trajectory-major (interleaved complex per trajectory)
-    void *b_parts = nullptr;  // parts x Mp x Dp bf16 (split state, K-major rows)
+    void *psi = nullptr;      // Mp x Dp fp32 (fp64 for int8), trajectory-major (interleaved complex per trajectory)
+    void *b_parts = nullptr;  // parts x Mp x Dp bf16 (split state, K-major rows); int8 slices for parts = 4
+    void *u_scale = nullptr;  // int8 form: Dp doubles, the power-of-two scale of each row of U (in u_parts)
+    void *b_scale = nullptr;  // int8 form: Mp doubles, the scale of each trajectory's slices (in b_parts)
     void *work = nullptr;     // FP64 scratch for building U (4 x D x D complex)
     void *tmaps = nullptr;    // device copy not needed: tensor maps are kernel parameters
     size_t bytes = 0;

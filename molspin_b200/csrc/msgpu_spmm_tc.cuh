@@ -26,26 +26,24 @@
 // 128 producer threads (thread = trajectory = TMEM lane) read their 8 real
 // values (Re/Im of the 4 rows), split each into three BF16 parts
 // x = x0 + x1 + x2 and store [x0 | x1 | x0 | x2] (16 TMEM columns) into a
-// TMEM slot; one thread issues, per (output, input) pair, three
+// TMEM slot.  Each output quartet owns 16 accumulator columns, [main (8) |
+// correction (8)], and one thread issues, per (output, input) pair, two
 // tcgen05.mma kind::f16 (M = 128 trajectories, N = 16, K = 16, A from TMEM,
-// B = the block in real form from shared memory):
-//     D_main += [x0 | x1] . [H0 ; H1]        (x0 H0 + x1 H1)
-//     D_corr += [x0 | x1] . [H1 ; H0]        (x0 H1 + x1 H0)
-//     D_corr += [x0 | x2] . [H2 ; H0]        (x0 H2 + x2 H0)
+// B from shared memory):
+//     [main | corr] += [x0 | x1] . [[H0 ; H1] | [H1 ; H0]]   (x0 H0 + x1 H1 | x0 H1 + x1 H0)
+//     [main | corr] += [x0 | x2] . [     0    | [H2 ; H0]]   (          0    | x0 H2 + x2 H0)
 // with H = H0 + H1 + H2 the BF16 split of the block's real form (8 x 8:
 // [[Re H, -Im H], [Im H, Re H]] acting on [Re x ; Im x]).  The dropped
 // products are 2^-24 of the result.  The correction products accumulate
 // apart from the main one: the FP32 accumulation of tcgen05.mma rounds
 // towards zero, and keeping the 2^-8-sized corrections out of the main
-// accumulator limits that bias to the main products' own.  The epilogue adds
-// the two accumulators (round to nearest), scales by s_j, stores U and the
-// per-trajectory FP64 partial of alpha_j = Re <v_j, U>.
+// accumulator limits that bias to the main products' own.  An output's first
+// MMA overwrites its 16 columns; the epilogue adds the two halves (round to
+// nearest), scales by s_j, stores U and the per-trajectory FP64 partial of
+// alpha_j = Re <v_j, U>.
 //
-// TMEM columns (CB = 4, 512 allocated): D_main [0, 128) + 8 pad, D_corr
-// [136, 264) + 8 pad, then 15 input slots of 16 columns.  An MMA of N = 16
-// writing an output's 8 columns also covers the next 8 (the B operand's
-// columns 8..15 are zero), hence the pads; the accumulators are cleared once
-// and every MMA accumulates.  CB = 3 allocates 256 columns (two CTAs per SM).
+// TMEM columns (CB = 4, 512 allocated): accumulators [0, 256), then 16 input
+// slots of 16 columns.  CB = 3 allocates 256 columns (two CTAs per SM).
 //
 // Every mbarrier wait is bounded; after the limit the kernel records status
 // bit 4, lets its own copies and MMAs drain (bounded), frees TMEM and
@@ -68,9 +66,7 @@ template <int CB>
 struct TcCfg {
     static constexpr int NQ = 1 << CB;             // output quartets per CTA
     static constexpr int Cols = CB == 4 ? 512 : 256;
-    static constexpr int DMain = 0;
-    static constexpr int DCorr = 8 * NQ + 8;
-    static constexpr int Slot0 = 2 * (8 * NQ + 8);
+    static constexpr int Slot0 = 16 * NQ;            // accumulators [0, Slot0): 16 columns per output
     static constexpr int NS = (Cols - Slot0) / 16;   // TMEM input slots
     static constexpr int NSTG = CB == 4 ? 12 : 8;    // shared-memory stages for translated inputs
     static constexpr int InBytes = 4 * kTcTraj * 8;  // one input quartet, 128 trajectories (4 KB)
@@ -78,9 +74,9 @@ struct TcCfg {
     static constexpr int OffOwn = 0;
     static constexpr int OffStage = OffOwn + NQ * InBytes;
     static constexpr int OffDiag = OffStage + NSTG * InBytes;
-    static constexpr int OffFlip = OffDiag + NQ * 3 * kTcB;
+    static constexpr int OffFlip = OffDiag + NQ * 2 * kTcB;
     static constexpr int NBar = 2 + 2 * NSTG + 2 * NS + 1;  // own, tables, stage full/empty, slot full/empty, done
-    __host__ __device__ static constexpr int off_bar(int P) { return OffFlip + P * 2 * 3 * kTcB; }
+    __host__ __device__ static constexpr int off_bar(int P) { return OffFlip + P * 2 * 2 * kTcB; }
     __host__ __device__ static constexpr int smem(int P) { return off_bar(P) + NBar * 8 + 16 /*abort, tmem slot*/; }
     static_assert(NS >= 4, "TMEM slots");
 };
@@ -141,13 +137,13 @@ __device__ __forceinline__ uint64_t tc_bdesc(uint32_t addr)
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(16 >> 3) << 17) |
                               (static_cast<uint32_t>(128 >> 4) << 24);
 
-__device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b)
+__device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b, uint32_t acc)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
         :
-        : "r"(d), "r"(a), "l"(b), "r"(kTcIdesc), "r"(1u)
+        : "r"(d), "r"(a), "l"(b), "r"(kTcIdesc), "r"(acc)
         : "memory");
 }
 
@@ -166,11 +162,13 @@ __device__ __forceinline__ void tc_st16(uint32_t taddr, const uint32_t (&v)[16])
         : "memory");
 }
 
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, uint32_t (&v)[8])
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16])
 {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                 : "r"(taddr));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
 }
 
 // Byte offset of element (n, k) in a 16 x 16 BF16 B operand (see tc_bdesc).
@@ -221,40 +219,43 @@ __device__ __forceinline__ void tc_expand(int type, const float2 *__restrict__ v
 
 // B-operand tables.  Entry e (src[e] = {value offset in float4 units, type} of
 // a block of the quartet form; offset < 0: no block, a zero operand) becomes
-// three 16 x 16 BF16 B operands (B1 = [H0; H1], B2 = [H1; H0], B3 = [H2; H0])
-// of the block's real form R[k][n]: k < 4 Re x_k, 4 <= k < 8 Im x_{k-4};
-// n < 4 Re y_n, 4 <= n < 8 Im y_{n-4}; columns 8..15 are zero.  One block of
-// 256 threads per entry, thread (n, k).
+// two 16 x 16 BF16 B operands of the block's real form R[k][n] (k < 4 Re x_k,
+// 4 <= k < 8 Im x_{k-4}; n < 4 Re y_n, 4 <= n < 8 Im y_{n-4}), with K rows
+// 0..7 against the first operand part and 8..15 against the second:
+//   BA: columns 0..7 [H0; H1] (main), columns 8..15 [H1; H0] (correction)
+//   BB: columns 0..7 zero,            columns 8..15 [H2; H0] (correction)
+// One block of 256 threads per entry, thread (n, k).
 __global__ void __launch_bounds__(256) k_tc_tables(const int2 *__restrict__ src, int nentries,
                                                    const float4 *__restrict__ qval, unsigned char *__restrict__ out)
 {
     const int e = blockIdx.x;
     if (e >= nentries) return;
     const int n = threadIdx.x >> 4, k = threadIdx.x & 15;
+    const int nn = n & 7;  // the real output component of column n
     float r = 0.f;
-    const int2 s = src[e];
-    if (n < 8 && s.x >= 0) {
+    const int2 s = src[e];  // s.x < 0: no such block (zero operand)
+    if (s.x >= 0) {
         float2 h[4][4];
         tc_expand(s.y, reinterpret_cast<const float2 *>(qval + s.x), h);
-        const int kk = k & 7, b = kk & 3, a = n & 3;
+        const int kk = k & 7, b = kk & 3, a = nn & 3;
         const float2 hab = h[a][b];
-        if (kk < 4) r = n < 4 ? hab.x : hab.y;  // Re x_b -> Re y_a: Re H; -> Im y_a: Im H
-        else r = n < 4 ? -hab.y : hab.x;        // Im x_b -> Re y_a: -Im H; -> Im y_a: Re H
+        if (kk < 4) r = nn < 4 ? hab.x : hab.y;  // Re x_b -> Re y_a: Re H; -> Im y_a: Im H
+        else r = nn < 4 ? -hab.y : hab.x;        // Im x_b -> Re y_a: -Im H; -> Im y_a: Re H
     }
     const __nv_bfloat16 p0 = __float2bfloat16_rn(r);
     const float r1 = r - __bfloat162float(p0);
     const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
     const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
-    const bool lo = k < 8;
-    unsigned char *o = out + static_cast<size_t>(e) * 3 * kTcB + tc_boff(n, k);
-    *reinterpret_cast<__nv_bfloat16 *>(o) = lo ? p0 : p1;             // B1 = [H0; H1]
-    *reinterpret_cast<__nv_bfloat16 *>(o + kTcB) = lo ? p1 : p0;      // B2 = [H1; H0]
-    *reinterpret_cast<__nv_bfloat16 *>(o + 2 * kTcB) = lo ? p2 : p0;  // B3 = [H2; H0]
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    const bool lo = k < 8, main_col = n < 8;
+    unsigned char *o = out + static_cast<size_t>(e) * 2 * kTcB + tc_boff(n, k);
+    *reinterpret_cast<__nv_bfloat16 *>(o) = main_col ? (lo ? p0 : p1) : (lo ? p1 : p0);  // BA
+    *reinterpret_cast<__nv_bfloat16 *>(o + kTcB) = main_col ? zero : (lo ? p2 : p0);     // BB
 }
 
 // U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
 // kTcThreads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
-//   tflip: [P][2 (output bit)][3] B operands; tdiag: [Q][3] B operands;
+//   tflip: [P][2 (output bit)][2] B operands; tdiag: [Q][2] B operands;
 //   base: quartet -> base row; {0, s2, s1, s1 + s2}: the rows of a quartet;
 //   w, sj, U, part start at the group's first trajectory; width = its
 //   trajectories (a multiple of 64); ldm = the row stride.
@@ -323,10 +324,10 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         if (tid == 160) {
             const uint32_t rowbytes = static_cast<uint32_t>(nvalid) * 8u;
             // B operands: every flip entry and this cube's diagonal blocks
-            tc_expect(bar_tab, static_cast<uint32_t>((P * 2 + NQ) * 3 * kTcB));
-            tc_bulk(sbase + Cfg::OffFlip, tflip, static_cast<uint32_t>(P * 2 * 3 * kTcB), bar_tab);
-            tc_bulk(sbase + Cfg::OffDiag, tdiag + static_cast<size_t>(q0) * 3 * kTcB,
-                    static_cast<uint32_t>(NQ * 3 * kTcB), bar_tab);
+            tc_expect(bar_tab, static_cast<uint32_t>((P * 2 + NQ) * 2 * kTcB));
+            tc_bulk(sbase + Cfg::OffFlip, tflip, static_cast<uint32_t>(P * 2 * 2 * kTcB), bar_tab);
+            tc_bulk(sbase + Cfg::OffDiag, tdiag + static_cast<size_t>(q0) * 2 * kTcB,
+                    static_cast<uint32_t>(NQ * 2 * kTcB), bar_tab);
             // the own cube: NQ quartets x 4 rows, kept for the alpha partial
             tc_expect(bar_own, static_cast<uint32_t>(NQ * 4) * rowbytes);
             for (int l = 0; l < NQ; ++l) {
@@ -361,6 +362,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         if (tid == 128) {
             bool ok = tc_wait(bar_tab, 0, abort);
             const uint32_t flip_s = sbase + Cfg::OffFlip, diag_s = sbase + Cfg::OffDiag;
+            uint32_t written = 0;  // bit o: output o's accumulator columns hold a value
             for (int j = 0; j < NI && ok; ++j) {
                 const int s = j % NS, r = j / NS;
                 if (!tc_wait(bar_tfull(s), r & 1, abort)) break;
@@ -368,21 +370,21 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 const uint32_t a01 = tmem + Cfg::Slot0 + 16 * s, a02 = a01 + 8;
                 const int g = j >> CB, l = j & (NQ - 1);
                 auto issue = [&](int o, uint32_t bt) {
-                    const uint32_t dm = tmem + Cfg::DMain + 8 * o, dc = tmem + Cfg::DCorr + 8 * o;
-                    tc_mma(dm, a01, tc_bdesc(bt));
-                    tc_mma(dc, a01, tc_bdesc(bt + kTcB));
-                    tc_mma(dc, a02, tc_bdesc(bt + 2 * kTcB));
+                    const uint32_t d = tmem + 16 * o;
+                    tc_mma(d, a01, tc_bdesc(bt), (written >> o) & 1u);  // the first one overwrites
+                    tc_mma(d, a02, tc_bdesc(bt + kTcB), 1u);
+                    written |= 1u << o;
                 };
                 if (g == 0) {
-                    issue(l, diag_s + l * 3 * kTcB);  // own block
+                    issue(l, diag_s + l * 2 * kTcB);  // own block
 #pragma unroll
                     for (int p = 0; p < CB; ++p) {
                         const int o = l ^ (1 << p);
-                        issue(o, flip_s + ((p * 2 + ((o >> p) & 1)) * 3) * kTcB);
+                        issue(o, flip_s + ((p * 2 + ((o >> p) & 1)) * 2) * kTcB);
                     }
                 } else {
                     const int p = CB + g - 1;
-                    issue(l, flip_s + ((p * 2 + ((q0 >> p) & 1)) * 3) * kTcB);
+                    issue(l, flip_s + ((p * 2 + ((q0 >> p) & 1)) * 2) * kTcB);
                 }
                 tc_commit(bar_tempty(s));
             }
@@ -394,14 +396,6 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         const int pair_off = (lane_traj & ~1) * 8;  // byte offset of the trajectory pair in a row
         const bool odd = lane_traj & 1;
         const uint32_t lane_addr = tmem + (static_cast<uint32_t>(32 * warp) << 16);
-        // clear both accumulators and their pads (every MMA accumulates); the
-        // first slot's fence and arrive below order this before any MMA
-        {
-            uint32_t z[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) z[i] = 0u;
-            for (int c0 = 0; c0 < Cfg::Slot0; c0 += 16) tc_st16(lane_addr + c0, z);
-        }
         // every wait's outcome is made uniform over the warp: the tcgen05.st/ld
         // and the shuffles below are warp-collective
         bool ok = __all_sync(0xffffffffu, tc_wait(bar_own, 0, abort));
@@ -469,13 +463,12 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
             const float sc = live ? static_cast<float>(sj[t]) : 0.f;
             double acc = 0.0;
             for (int o = 0; o < NQ; ++o) {
-                uint32_t dm[8], dc[8];
-                tc_ld8(lane_addr + Cfg::DMain + 8 * o, dm);
-                tc_ld8(lane_addr + Cfg::DCorr + 8 * o, dc);
+                uint32_t dv[16];  // [main (8) | correction (8)]
+                tc_ld16(lane_addr + 16 * o, dv);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 float y[8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) y[i] = (__uint_as_float(dc[i]) + __uint_as_float(dm[i])) * sc;
+                for (int i = 0; i < 8; ++i) y[i] = (__uint_as_float(dv[8 + i]) + __uint_as_float(dv[i])) * sc;
                 // own input rows of this output (for alpha), pair-planar
                 const unsigned char *own = sm + Cfg::OffOwn + o * Cfg::InBytes;
                 const int b = base[q0 + o];

@@ -177,11 +177,12 @@ class HSPropagatorB200:
         return out.T
 
     # ------------------------------------------------------------ propagation
-    PRECISIONS = {"c128": L.PREC_C128, "c64": L.PREC_C64, "bf16x3": L.PREC_BF16X3, "bf16x6": L.PREC_BF16X6}
+    PRECISIONS = {"c128": L.PREC_C128, "c64": L.PREC_C64, "bf16x3": L.PREC_BF16X3, "bf16x6": L.PREC_BF16X6,
+                  "int8x4": L.PREC_INT8X4}
 
     def propagate(self, times: np.ndarray, krylov: int, precision: str = "c128", step_offset: int = 0,
                   accumulate: bool = False, recurrence: int = L.REC_AUTO, propagator: str = "krylov"):
-        """propagator "krylov" (precision c128 | c64), "dense" (bf16x3 | bf16x6,
+        """propagator "krylov" (precision c128 | c64), "dense" (bf16x3 | bf16x6 | int8x4,
         tensor cores), "taylor" (c128; the reference's autoexpm) or "rk4" (c128, explicit)."""
         t = np.ascontiguousarray(times, dtype=np.float64)
         prop = {"krylov": L.PROP_KRYLOV, "dense": L.PROP_DENSE, "taylor": L.PROP_TAYLOR, "rk4": L.PROP_RK4}[propagator]

@@ -4,12 +4,20 @@ A request is one HSGeneral stochastic yield solve -- one radical-pair system
 at one field orientation, as one RunSection step of the reference
 (RunSection::Run -> TaskHSGeneral::RunLocal, main.cpp:651-678).  The engine
 admits requests as they arrive, first-fit against a device-memory budget and
-a number of slots.  Each admitted request gets its own msgpu context (its
+a number of slots.  Each admitted request runs on its own msgpu context (its
 own CUDA stream; the budget it reserved is enforced by the context), and
 worker threads drive the C ABI with the GIL released, so requests that
 arrive while others run are admitted as soon as slots and memory free up
 and their kernels overlap on the device.  Latency (arrival -> yields on the
 host) is reported as p50/p99 beside throughput.
+
+Contexts are pooled by request shape (dimension, trajectories, Krylov
+dimension, steps): a finished request's context, with its device buffers,
+its quartet-form and SpMM tuning, serves the next request of that shape, so
+a steady stream allocates and frees no device memory (a cudaFree waits for
+the whole device, i.e. for every other request's kernels).  Idle contexts
+keep their reservation and are destroyed only when an admission needs the
+memory.
 
 Results do not depend on the mix: noise is counter-based Philox keyed by the
 request's seed and each trajectory/step, reductions are two-phase in a fixed
@@ -81,38 +89,96 @@ class ServingEngine:
         self.slots = slots
         self.precision = precision
         self._lock = threading.Condition()
-        self._reserved = 0
+        self._reserved = 0   # running requests plus idle pooled contexts
         self._running = 0
+        self._idle: dict[tuple, list[tuple[HSPropagatorB200, int]]] = {}  # shape -> [(context, reserved)]
         self.max_concurrency = 0
         self.peak_reserved = 0
+        self.contexts_created = 0
+        self.contexts_reused = 0
 
-    def solve(self, req: Request, budget: int = 0) -> np.ndarray:
-        """One request on its own context; returns the ensemble yields."""
+    @staticmethod
+    def shape(w: Workload) -> tuple:
+        return (w.system.dim, w.M, w.krylov, w.steps)
+
+    def _run(self, p: HSPropagatorB200, req: Request) -> np.ndarray:
         w = req.workload
         s = w.system
         F = s.trace_samples(w.M, w.seed)
-        with HSPropagatorB200(self.device, budget) as p:
-            p.set_hamiltonian(*s.hamiltonian_csr())
-            p.set_reaction(kappa=s.kappa())
-            p.set_electron_pair(*s.electron_strides())
-            p.set_observables([(op, rate) for _, op, rate in s.observables()])
-            if s.st_rate > 0.0:
-                p.set_noise(s.st_rate, L.NOISE_PHILOX, req.seed)
-            p.set_factors(F)
-            p.propagate(w.times(), w.krylov, self.precision)
-            _, ens = p.yields()
+        p.set_hamiltonian(*s.hamiltonian_csr())
+        p.set_reaction(kappa=s.kappa())
+        p.set_electron_pair(*s.electron_strides())
+        p.set_observables([(op, rate) for _, op, rate in s.observables()])
+        # every input is set on every request: a pooled context keeps the last one's
+        if s.st_rate > 0.0:
+            p.set_noise(s.st_rate, L.NOISE_PHILOX, req.seed)
+        else:
+            p.set_noise(0.0, L.NOISE_NONE)
+        p.set_factors(F)
+        p.propagate(w.times(), w.krylov, self.precision)
+        _, ens = p.yields()
         return ens
 
-    def _worker(self, req: Request, res: Result, t0: float):
+    def solve(self, req: Request, budget: int = 0) -> np.ndarray:
+        """One request on a context of its own (created and destroyed here);
+        returns the ensemble yields."""
+        with HSPropagatorB200(self.device, budget) as p:
+            return self._run(p, req)
+
+    def solve_pooled(self, req: Request, budget: int, ctx):
+        """One request on a pooled context (a new one when ctx is None);
+        returns (ensemble yields, the context to keep for the pool)."""
+        if ctx is None:
+            ctx = HSPropagatorB200(self.device, budget)
         try:
-            res.yields = self.solve(req, res.reserved)
+            return self._run(ctx, req), ctx
+        except Exception:
+            ctx.close()
+            raise
+
+    def _worker(self, req: Request, res: Result, t0: float, ctx):
+        try:
+            res.yields, ctx = self.solve_pooled(req, res.reserved, ctx)
         except Exception as e:  # noqa: BLE001 -- reported per request
             res.error = str(e)
+            ctx = None
         res.finished = time.perf_counter() - t0
         with self._lock:
-            self._reserved -= res.reserved
+            if ctx is not None:
+                self._idle.setdefault(self.shape(req.workload), []).append((ctx, res.reserved))
+            else:
+                self._reserved -= res.reserved
             self._running -= 1
             self._lock.notify_all()
+
+    def _evict(self, need: int) -> list[tuple[HSPropagatorB200, int]]:
+        """Idle contexts to destroy (largest first) so that `need` more bytes fit;
+        called with the lock held, the contexts are closed by the caller."""
+        out = []
+        pool = sorted(((r, k, i) for k, lst in self._idle.items() for i, (_, r) in enumerate(lst)), reverse=True)
+        freed, take = 0, []
+        for r, k, i in pool:
+            if self._reserved - freed + need <= self.budget:
+                break
+            take.append((k, i))
+            freed += r
+        if self._reserved - freed + need > self.budget:
+            return out  # evicting everything idle would not make room: wait for running requests
+        for k, i in sorted(take, key=lambda x: -x[1]):
+            out.append(self._idle[k].pop(i))
+        for k in [k for k, lst in self._idle.items() if not lst]:
+            del self._idle[k]
+        self._reserved -= freed
+        return out
+
+    def close(self):
+        """Destroys the idle pooled contexts."""
+        with self._lock:
+            idle = [c for lst in self._idle.values() for c in lst]
+            self._idle.clear()
+            self._reserved -= sum(r for _, r in idle)
+        for ctx, _ in idle:
+            ctx.close()
 
     def serve(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         """Run a request stream; arrivals are honoured in wall-clock time when
@@ -135,23 +201,40 @@ class ServingEngine:
                     if not results[order[i].rid].error:
                         waiting.append(order[i])
                     i += 1
-                # first fit: admit every waiting request that fits the free slots and memory
+                # first fit: admit every waiting request that fits the free slots
+                # and memory, on an idle pooled context of its shape if there is one
                 k = 0
                 while k < len(waiting) and self._running < self.slots:
                     req = waiting[k]
                     res = results[req.rid]
-                    if self._reserved + res.reserved <= self.budget:
-                        waiting.pop(k)
-                        self._reserved += res.reserved
-                        self._running += 1
-                        self.max_concurrency = max(self.max_concurrency, self._running)
-                        self.peak_reserved = max(self.peak_reserved, self._reserved)
-                        res.admitted = now
-                        th = threading.Thread(target=self._worker, args=(req, res, t0), daemon=True)
-                        th.start()
-                        threads.append(th)
+                    ctx = None
+                    pooled = self._idle.get(self.shape(req.workload))
+                    if pooled:
+                        ctx, res.reserved = pooled.pop()
+                        self.contexts_reused += 1
                     else:
-                        k += 1
+                        if self._reserved + res.reserved > self.budget:
+                            evicted = self._evict(res.reserved)
+                            if evicted:
+                                self._lock.release()
+                                try:
+                                    for c, _ in evicted:
+                                        c.close()
+                                finally:
+                                    self._lock.acquire()
+                        if self._reserved + res.reserved > self.budget:
+                            k += 1
+                            continue
+                        self._reserved += res.reserved
+                        self.contexts_created += 1
+                    waiting.pop(k)
+                    self._running += 1
+                    self.max_concurrency = max(self.max_concurrency, self._running)
+                    self.peak_reserved = max(self.peak_reserved, self._reserved)
+                    res.admitted = now
+                    th = threading.Thread(target=self._worker, args=(req, res, t0, ctx), daemon=True)
+                    th.start()
+                    threads.append(th)
                 if i >= len(order) and not waiting and self._running == 0:
                     break
                 timeout = None
@@ -160,6 +243,7 @@ class ServingEngine:
                 self._lock.wait(timeout=timeout if timeout is not None else 1.0)
         for th in threads:
             th.join()
+        self.close()
         return [results[r.rid] for r in requests]
 
 

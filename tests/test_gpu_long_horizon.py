@@ -54,7 +54,8 @@ def test_precision_form_over_2000_steps():
 
 
 # (precision, per-trajectory tolerance, ensemble tolerance)
-DENSE_TOL = [("bf16x3", 1.5e-4, 1.2e-4), ("bf16x6", 2e-5, 1.6e-5)]
+# int8x4 (exact int32 accumulation, FP64 state) is held to the precision forms' 1e-6 target
+DENSE_TOL = [("bf16x3", 1.5e-4, 1.2e-4), ("bf16x6", 2e-5, 1.6e-5), ("int8x4", 1e-6, 1e-6)]
 
 
 @pytest.fixture(scope="module")

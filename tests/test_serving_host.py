@@ -1,5 +1,6 @@
 """Host logic of the serving engine without a GPU: admission against slots
-and the memory budget, first-fit order, arrival times and the summary."""
+and the memory budget, first-fit order, arrival times, the context pool and
+the summary."""
 import threading
 import time
 
@@ -7,6 +8,17 @@ import numpy as np
 
 from molspin_b200 import serving as SV
 from molspin_b200 import systems as S
+
+
+class FakeCtx:
+    """Stands in for a device context: records its budget and whether it was closed."""
+    def __init__(self, budget):
+        self.budget = budget
+        self.closed = False
+        self.served = 0
+
+    def close(self):
+        self.closed = True
 
 
 class FakeEngine(SV.ServingEngine):
@@ -17,16 +29,22 @@ class FakeEngine(SV.ServingEngine):
         self.peak_active = 0
         self.lock = threading.Lock()
         self.started = []
+        self.ctxs = []
 
-    def solve(self, req, budget=0):
+    def solve_pooled(self, req, budget, ctx):
         with self.lock:
+            if ctx is None:
+                ctx = FakeCtx(budget)
+                self.ctxs.append(ctx)
+            assert not ctx.closed
+            ctx.served += 1
             self.active += 1
             self.peak_active = max(self.peak_active, self.active)
             self.started.append(req.rid)
         time.sleep(self.work_s)
         with self.lock:
             self.active -= 1
-        return np.array([float(req.rid)])
+        return np.array([float(req.rid)]), ctx
 
 
 def _reqs(n, arrivals, nuclei=(6, 7)):
@@ -82,3 +100,28 @@ def test_footprint_grows_with_dimension():
     small = SV.footprint(S.serving_request(0, nuclei=(6, 6), steps=10))
     big = SV.footprint(S.serving_request(0, nuclei=(12, 12), steps=10))
     assert big > 10 * small
+
+
+def test_contexts_are_pooled_by_shape_and_closed_at_the_end():
+    # ten requests of one shape through two slots: contexts are reused, never
+    # more of them than slots, and all are closed when the stream ends
+    reqs = [SV.Request(i, 0.0, S.serving_request(0, nuclei=(7, 7), steps=10), seed=i) for i in range(10)]
+    eng = FakeEngine(hbm_budget=1 << 40, slots=2, work_s=0.01)
+    res = eng.serve(reqs, realtime=False)
+    assert all(not r.error for r in res)
+    assert eng.contexts_created == len(eng.ctxs) <= 2 and eng.contexts_reused == 10 - eng.contexts_created
+    assert sum(c.served for c in eng.ctxs) == 10 and all(c.closed for c in eng.ctxs)
+    assert eng._reserved == 0
+
+
+def test_idle_contexts_are_evicted_when_memory_is_needed():
+    # a small-shape context left idle must give way to a large request that
+    # would not fit beside it
+    small = SV.Request(0, 0.0, S.serving_request(0, nuclei=(6, 6), steps=10), seed=0)
+    large = SV.Request(1, 0.05, S.serving_request(1, nuclei=(9, 9), steps=10), seed=1)
+    fs, fl = SV.footprint(small.workload), SV.footprint(large.workload)
+    eng = FakeEngine(hbm_budget=fl + fs // 2, slots=2, work_s=0.01)
+    res = eng.serve([small, large], realtime=True)
+    assert all(not r.error for r in res), [r.error for r in res]
+    assert eng.peak_reserved <= eng.budget
+    assert eng.ctxs[0].closed and eng.contexts_created == 2
