@@ -634,6 +634,13 @@ def run_batching(args):
     el = _max_over_ranks(sum(ms[args.warmup:]), world)
     st = bt.stats()
     Mtot = sum(w.M for w in ws)
+    # per-system routes and, for the streamed systems, the SpMM each one's tuner picked
+    infos = [bt.system_info(i) for i in range(len(ws))]
+    picks = {}
+    for i, inf in enumerate(infos):
+        if inf["streamed"]:
+            key = f"variant {inf['spmm_variant']} tile {inf['spmm_tile']} groups {inf['traj_groups']}"
+            picks.setdefault(key, []).append(ws[i].system.dim)
     bt.close()
     # whole-batch HBM roofline with the minimal fused Krylov traffic (4m+1) D c per traj-step
     # (complex64, c = 8 B); the persistent kernel keeps small systems on chip, so this is the
@@ -654,6 +661,8 @@ def run_batching(args):
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None,
                      "traffic": None, "peak_kind": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clk, "e2e": None, "gpu_launches": launches,
+        "routes": {"persistent": sum(not i["streamed"] for i in infos), "streamed": sum(i["streamed"] for i in infos),
+                   "streamed_spmm_picks": {k: sorted(v) for k, v in picks.items()}},
         "launch_note": "per bench step: one graph replay of the persistent k_batch launch (systems below D=2048) "
                        "plus the streamed path's kernels for the larger systems", "cpu_baseline": None})
 

@@ -288,6 +288,19 @@ long long msgpu_batch_launch_count(const msgpu_batch *batch);
 /* Number of kernels this context launched since creation. */
 long long msgpu_launch_count(const msgpu_ctx *ctx);
 
+/* The complex64 SpMM this context's autotuner picked for its current
+ * trajectory block: *variant in the numbering of MSGPU_OPT_SPMM_VARIANT,
+ * *tile the quartets per CTA, *groups the trajectory groups of the step;
+ * all -1 before the first complex64 streamed run.  No counterpart in the
+ * reference (a tuning report). */
+int msgpu_spmm_choice(const msgpu_ctx *ctx, int *variant, int *tile, int *groups);
+
+/* System i of a batch: *streamed = 1 when it runs the streamed single-system
+ * path on its own context (dimension >= 2048), 0 inside the persistent
+ * launch; for a streamed system the SpMM its own tuner picked
+ * (msgpu_spmm_choice), else -1.  No counterpart in the reference. */
+int msgpu_batch_system_info(const msgpu_batch *batch, int system, int *streamed, int *variant, int *tile, int *groups);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (for example an embedding host framework whose memory pool owns
  * all device memory, or code on a latency-critical path that must not take

@@ -113,6 +113,8 @@ def _load() -> C.CDLL:
         "msgpu_batch_fetch_yields": (I, [P, I, pD, pD]),
         "msgpu_batch_stats": (I, [P, pD, pI, pI]),
         "msgpu_batch_launch_count": (C.c_longlong, [P]),
+        "msgpu_spmm_choice": (I, [P, pI, pI, pI]),
+        "msgpu_batch_system_info": (I, [P, I, pI, pI, pI, pI]),
         "msgpu_krylov_step_noalloc": (I, [I, P, P, P, D, I, P, P, D, I, P]),
         "msgpu_host_build_hamiltonian": (C.c_longlong, [I, pI, I, pI, pD, I, pI, pI, pD, pI, pI, pD]),
         "msgpu_host_trace_samples": (I, [D, pD, I, I, I, pD]),

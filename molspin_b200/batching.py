@@ -91,6 +91,13 @@ class BatchB200:
     def launch_count(self) -> int:
         return int(L.lib.msgpu_batch_launch_count(self.b))
 
+    def system_info(self, i: int) -> dict:
+        """Route of system i (streamed or persistent) and, when streamed, the
+        SpMM its context's tuner picked."""
+        st, v, t, g = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        self._check(L.lib.msgpu_batch_system_info(self.b, int(i), C.byref(st), C.byref(v), C.byref(t), C.byref(g)))
+        return {"streamed": bool(st.value), "spmm_variant": v.value, "spmm_tile": t.value, "traj_groups": g.value}
+
     def stats(self):
         ms = C.c_double(0.0)
         th = C.c_int(0)

@@ -1538,16 +1538,15 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
     const unsigned char *tdiag = tflip + static_cast<size_t>(2 * P) * 2 * kTcB;
     const dim3 grid(Q >> cb, ceil_div(width, kTcTraj));
     int *status = static_cast<int *>(c->status.p);
-    const int *base = static_cast<const int *>(c->qbase.p);
     if (cb == 4) {
         const int smem = TcCfg<4>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<4>), smem);
-        k_lanczos_apply_tc<4><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
+        k_lanczos_apply_tc<4><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     } else {
         const int smem = TcCfg<3>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<3>), smem);
-        k_lanczos_apply_tc<3><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, base, c->s1, c->s2, w, s, U, part, c->ldm,
+        k_lanczos_apply_tc<3><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     }
 }
@@ -2210,6 +2209,16 @@ int msgpu_fetch_values(msgpu_ctx *c, double *values)
     if (!c) return MSGPU_ERR_INVALID;
     if (!c->have_integrals || !values) return fail(c, MSGPU_ERR_STATE, "no values: run first");
     std::copy(c->last_values.begin(), c->last_values.end(), values);
+    return MSGPU_OK;
+}
+
+int msgpu_spmm_choice(const msgpu_ctx *c, int *variant, int *tile, int *groups)
+{
+    if (!c) return MSGPU_ERR_INVALID;
+    const bool tuned = c->q_tile > 0;
+    if (variant) *variant = tuned ? c->q_variant : -1;
+    if (tile) *tile = tuned ? c->q_tile : -1;
+    if (groups) *groups = tuned ? traj_groups(c) : -1;
     return MSGPU_OK;
 }
 

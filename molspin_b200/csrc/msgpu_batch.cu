@@ -529,6 +529,18 @@ long long msgpu_batch_launch_count(const msgpu_batch *b)
     return n;
 }
 
+int msgpu_batch_system_info(const msgpu_batch *b, int i, int *streamed, int *variant, int *tile, int *groups)
+{
+    if (!b || i < 0 || i >= static_cast<int>(b->sys.size())) return MSGPU_ERR_INVALID;
+    const BatchSystem &s = b->sys[i];
+    if (streamed) *streamed = s.ctx ? 1 : 0;
+    if (s.ctx) return msgpu_spmm_choice(s.ctx, variant, tile, groups);
+    if (variant) *variant = -1;
+    if (tile) *tile = -1;
+    if (groups) *groups = -1;
+    return MSGPU_OK;
+}
+
 int msgpu_batch_stats(const msgpu_batch *b, double *last_run_ms, int *team_threshold, int *ctas_per_sm)
 {
     if (!b) return MSGPU_ERR_INVALID;

@@ -54,6 +54,8 @@
 
 #include <cstdint>
 
+#include "msgpu_device.cuh"
+
 namespace msgpu {
 
 constexpr int kTcTraj = 128;            // trajectories per CTA (TMEM lanes, MMA M)
@@ -256,13 +258,14 @@ __global__ void __launch_bounds__(256) k_tc_tables(const int2 *__restrict__ src,
 // U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
 // kTcThreads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
 //   tflip: [P][2 (output bit)][2] B operands; tdiag: [Q][2] B operands;
-//   base: quartet -> base row; {0, s2, s1, s1 + s2}: the rows of a quartet;
+//   quartet_base(q, s1, s2) + {0, s2, s1, s1 + s2}: the rows of quartet q (arithmetic:
+//   the issuing thread must not wait on a load per input);
 //   w, sj, U, part start at the group's first trajectory; width = its
 //   trajectories (a multiple of 64); ldm = the row stride.
 template <int CB>
 __global__ void __launch_bounds__(kTcThreads, 1)
-k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char *__restrict__ tdiag, int P,
-                   const int *__restrict__ base, int s1, int s2, const float2 *__restrict__ w,
+k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char *__restrict__ tdiag, int P, int s1,
+                   int s2, const float2 *__restrict__ w,
                    const double *__restrict__ sj, float2 *__restrict__ U, double *__restrict__ part, int ldm,
                    int width, int *__restrict__ status)
 {
@@ -331,7 +334,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
             // the own cube: NQ quartets x 4 rows, kept for the alpha partial
             tc_expect(bar_own, static_cast<uint32_t>(NQ * 4) * rowbytes);
             for (int l = 0; l < NQ; ++l) {
-                const int b = base[q0 + l];
+                const int b = quartet_base(q0 + l, s1, s2);
                 for (int a = 0; a < 4; ++a)
                     tc_bulk(sbase + Cfg::OffOwn + (l * 4 + a) * kTcTraj * 8, w + static_cast<size_t>(b + off[a]) * ldm + t0,
                             rowbytes, bar_own);
@@ -342,7 +345,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 const int k = j - NQ, s = k % NSTG, r = k / NSTG;
                 if (!tc_wait(bar_sempty(s), (r & 1) ^ 1, abort)) break;
                 tc_expect(bar_sfull(s), 4u * rowbytes);
-                const int b = base[input_quartet(j)];
+                const int b = quartet_base(input_quartet(j), s1, s2);
                 for (int a = 0; a < 4; ++a)
                     tc_bulk(sbase + Cfg::OffStage + s * Cfg::InBytes + a * kTcTraj * 8,
                             w + static_cast<size_t>(b + off[a]) * ldm + t0, rowbytes, bar_sfull(s));
@@ -399,57 +402,71 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         // every wait's outcome is made uniform over the warp: the tcgen05.st/ld
         // and the shuffles below are warp-collective
         bool ok = __all_sync(0xffffffffu, tc_wait(bar_own, 0, abort));
-        for (int j = 0; j < NI && ok; ++j) {
-            const unsigned char *src;
-            if (j < NQ) {
-                src = sm + Cfg::OffOwn + j * Cfg::InBytes;
-            } else {
-                const int k = j - NQ;
-                if (!__all_sync(0xffffffffu, tc_wait(bar_sfull(k % NSTG), (k / NSTG) & 1, abort))) {
+        // Inputs go in pairs (NI is even): both are split and stored before one
+        // tcgen05.wait::st, so a TMEM store round trip is paid once per pair.
+        for (int j0 = 0; j0 < NI && ok; j0 += 2) {
+            uint32_t pk[2][16];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = j0 + h;
+                const unsigned char *src;
+                if (j < NQ) {
+                    src = sm + Cfg::OffOwn + j * Cfg::InBytes;
+                } else {
+                    const int k = j - NQ;
+                    if (!__all_sync(0xffffffffu, tc_wait(bar_sfull(k % NSTG), (k / NSTG) & 1, abort))) {
+                        ok = false;
+                        break;
+                    }
+                    src = sm + Cfg::OffStage + (k % NSTG) * Cfg::InBytes;
+                }
+                float x[8];  // Re rows 0..3, Im rows 0..3
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const float4 v = *reinterpret_cast<const float4 *>(src + a * kTcTraj * 8 + pair_off);
+                    x[a] = odd ? v.y : v.x;
+                    x[4 + a] = odd ? v.w : v.z;
+                }
+                if (j >= NQ) {
+                    __syncwarp();
+                    if ((tid & 31) == 0) tc_arrive(bar_sempty((j - NQ) % NSTG));
+                }
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    __nv_bfloat16 h0[2], h1[2], h2[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const float xv = x[2 * c + e];
+                        h0[e] = __float2bfloat16_rn(xv);
+                        const float r1 = xv - __bfloat162float(h0[e]);
+                        h1[e] = __float2bfloat16_rn(r1);
+                        h2[e] = __float2bfloat16_rn(r1 - __bfloat162float(h1[e]));
+                    }
+                    pk[h][c] = tc_pack(h0[0], h0[1]);
+                    pk[h][4 + c] = tc_pack(h1[0], h1[1]);
+                    pk[h][8 + c] = pk[h][c];
+                    pk[h][12 + c] = tc_pack(h2[0], h2[1]);
+                }
+            }
+            if (!ok) break;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = j0 + h, s = j % NS, r = j / NS;
+                if (!__all_sync(0xffffffffu, tc_wait(bar_tempty(s), (r & 1) ^ 1, abort))) {
                     ok = false;
                     break;
                 }
-                src = sm + Cfg::OffStage + (k % NSTG) * Cfg::InBytes;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                tc_st16(lane_addr + Cfg::Slot0 + 16 * s, pk[h]);
             }
-            float x[8];  // Re rows 0..3, Im rows 0..3
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const float4 v = *reinterpret_cast<const float4 *>(src + a * kTcTraj * 8 + pair_off);
-                x[a] = odd ? v.y : v.x;
-                x[4 + a] = odd ? v.w : v.z;
-            }
-            if (j >= NQ) {
-                __syncwarp();
-                if ((tid & 31) == 0) tc_arrive(bar_sempty((j - NQ) % NSTG));
-            }
-            uint32_t pk[16];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                __nv_bfloat16 h0[2], h1[2], h2[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const float xv = x[2 * c + e];
-                    h0[e] = __float2bfloat16_rn(xv);
-                    const float r1 = xv - __bfloat162float(h0[e]);
-                    h1[e] = __float2bfloat16_rn(r1);
-                    h2[e] = __float2bfloat16_rn(r1 - __bfloat162float(h1[e]));
-                }
-                pk[c] = tc_pack(h0[0], h0[1]);
-                pk[4 + c] = tc_pack(h1[0], h1[1]);
-                pk[8 + c] = pk[c];
-                pk[12 + c] = tc_pack(h2[0], h2[1]);
-            }
-            const int s = j % NS, r = j / NS;
-            if (!__all_sync(0xffffffffu, tc_wait(bar_tempty(s), (r & 1) ^ 1, abort))) {
-                ok = false;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            tc_st16(lane_addr + Cfg::Slot0 + 16 * s, pk);
+            if (!ok) break;
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
-            if ((tid & 31) == 0) tc_arrive(bar_tfull(s));
+            if ((tid & 31) == 0) {
+                tc_arrive(bar_tfull(j0 % NS));
+                tc_arrive(bar_tfull((j0 + 1) % NS));
+            }
         }
         // ------------------------------------------------------------ epilogue
         bool done = tc_wait(bar_done, 0, abort);
@@ -471,7 +488,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 for (int i = 0; i < 8; ++i) y[i] = (__uint_as_float(dv[8 + i]) + __uint_as_float(dv[i])) * sc;
                 // own input rows of this output (for alpha), pair-planar
                 const unsigned char *own = sm + Cfg::OffOwn + o * Cfg::InBytes;
-                const int b = base[q0 + o];
+                const int b = quartet_base(q0 + o, s1, s2);
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const float4 v = *reinterpret_cast<const float4 *>(own + a * kTcTraj * 8 + pair_off);

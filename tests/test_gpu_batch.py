@@ -36,7 +36,9 @@ def _run(entries, times, krylov, chunks=None, tune=False):
             for k, stop in enumerate(chunks):
                 bt.run(times[start:stop + 1], krylov, step_offset=start, accumulate=k > 0)
                 start = stop
-        return [bt.yields(i) for i in idx], bt.stats()
+        stats = bt.stats()
+        stats["systems"] = [bt.system_info(i) for i in idx]
+        return [bt.yields(i) for i in idx], stats
 
 
 def test_batch_matches_oracle():
@@ -74,7 +76,13 @@ def test_batch_streams_large_systems_through_the_single_system_path():
     entries = [_systems()[0], (big, 45, 14)]
     times = S.time_grid(12.0, 1.0)
     m = 10
-    out, _ = _run(entries, times, m, tune=True)
+    out, stats = _run(entries, times, m, tune=True)
+    # the small system runs in the persistent launch; the large one on its own
+    # context, whose tuner picked an SpMM variant, tile and trajectory grouping
+    small_info, big_info = stats["systems"]
+    assert not small_info["streamed"] and small_info["spmm_variant"] == -1
+    assert big_info["streamed"] and big_info["spmm_variant"] >= 0 and big_info["spmm_tile"] > 0
+    assert big_info["traj_groups"] >= 1
     F = big.trace_samples(45, 14.0)
     with hs.HSPropagatorB200(0) as p:
         p.set_hamiltonian(*big.hamiltonian_csr())
