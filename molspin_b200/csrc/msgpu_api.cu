@@ -1541,12 +1541,12 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
     if (cb == 4) {
         const int smem = TcCfg<4>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<4>), smem);
-        k_lanczos_apply_tc<4><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
+        k_lanczos_apply_tc<4><<<grid, TcCfg<4>::Threads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     } else {
         const int smem = TcCfg<3>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<3>), smem);
-        k_lanczos_apply_tc<3><<<grid, kTcThreads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
+        k_lanczos_apply_tc<3><<<grid, TcCfg<3>::Threads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
                                                               width, status);
     }
 }

@@ -59,7 +59,6 @@
 namespace msgpu {
 
 constexpr int kTcTraj = 128;            // trajectories per CTA (TMEM lanes, MMA M)
-constexpr int kTcThreads = 192;         // warps 0-3 producers/epilogue, 4 MMA issuer, 5 TMA issuer
 constexpr int kTcB = 512;               // bytes of one 16 x 16 BF16 B operand
 constexpr int kTcMaxBits = 14;          // quartet bits P (D <= 65536)
 constexpr uint32_t kTcWait = 1u << 23;  // iterations of a bounded mbarrier wait
@@ -67,6 +66,10 @@ constexpr uint32_t kTcWait = 1u << 23;  // iterations of a bounded mbarrier wait
 template <int CB>
 struct TcCfg {
     static constexpr int NQ = 1 << CB;             // output quartets per CTA
+    // producer warpgroups (each of 4 warps covers the 128 TMEM lanes; they take
+    // alternate input pairs and alternate outputs), then the MMA and TMA warps
+    static constexpr int G = CB == 4 ? 4 : 2;
+    static constexpr int Threads = 32 * (4 * G + 2);
     static constexpr int Cols = CB == 4 ? 512 : 256;
     static constexpr int Slot0 = 16 * NQ;            // accumulators [0, Slot0): 16 columns per output
     static constexpr int NS = (Cols - Slot0) / 16;   // TMEM input slots
@@ -256,21 +259,23 @@ __global__ void __launch_bounds__(256) k_tc_tables(const int2 *__restrict__ src,
 }
 
 // U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
-// kTcThreads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
+// TcCfg<CB>::Threads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
 //   tflip: [P][2 (output bit)][2] B operands; tdiag: [Q][2] B operands;
 //   quartet_base(q, s1, s2) + {0, s2, s1, s1 + s2}: the rows of quartet q (arithmetic:
 //   the issuing thread must not wait on a load per input);
 //   w, sj, U, part start at the group's first trajectory; width = its
 //   trajectories (a multiple of 64); ldm = the row stride.
 template <int CB>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(TcCfg<CB>::Threads, 1)
 k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char *__restrict__ tdiag, int P, int s1,
                    int s2, const float2 *__restrict__ w,
                    const double *__restrict__ sj, float2 *__restrict__ U, double *__restrict__ part, int ldm,
                    int width, int *__restrict__ status)
 {
     using Cfg = TcCfg<CB>;
-    constexpr int NQ = Cfg::NQ, NS = Cfg::NS, NSTG = Cfg::NSTG;
+    constexpr int NQ = Cfg::NQ, NS = Cfg::NS, NSTG = Cfg::NSTG, G = Cfg::G;
+    constexpr int kMmaWarp = 4 * G, kTmaWarp = 4 * G + 1;
+    __shared__ double s_alpha[G][kTcTraj];  // per-group alpha partials, summed in group order
     extern __shared__ __align__(128) unsigned char tc_raw[];
     unsigned char *sm = tc_raw;
     const uint32_t sbase = tc_smem(sm);
@@ -322,9 +327,9 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         return g == 0 ? q0 + l : (q0 + l) ^ (1 << (CB + g - 1));
     };
 
-    if (warp == 5) {
+    if (warp == kTmaWarp) {
         // ------------------------------------------------------------ TMA issuer
-        if (tid == 160) {
+        if (tid == 32 * kTmaWarp) {
             const uint32_t rowbytes = static_cast<uint32_t>(nvalid) * 8u;
             // B operands: every flip entry and this cube's diagonal blocks
             tc_expect(bar_tab, static_cast<uint32_t>((P * 2 + NQ) * 2 * kTcB));
@@ -360,9 +365,9 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
             for (uint32_t it = 0; it < kTcWait && !tc_try(bar_tab, 0); ++it) {
             }
         }
-    } else if (warp == 4) {
+    } else if (warp == kMmaWarp) {
         // ------------------------------------------------------------ MMA issuer
-        if (tid == 128) {
+        if (tid == 32 * kMmaWarp) {
             bool ok = tc_wait(bar_tab, 0, abort);
             const uint32_t flip_s = sbase + Cfg::OffFlip, diag_s = sbase + Cfg::OffDiag;
             uint32_t written = 0;  // bit o: output o's accumulator columns hold a value
@@ -395,16 +400,17 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         }
     } else {
         // ------------------------------------------------------------ producers
-        const int lane_traj = tid;                  // TMEM lane = trajectory in the tile
-        const int pair_off = (lane_traj & ~1) * 8;  // byte offset of the trajectory pair in a row
+        const int grp = warp >> 2, wq = warp & 3;       // warpgroup, and its warp's TMEM lane quarter
+        const int lane_traj = 32 * wq + (tid & 31);     // TMEM lane = trajectory in the tile
+        const int pair_off = (lane_traj & ~1) * 8;      // byte offset of the trajectory pair in a row
         const bool odd = lane_traj & 1;
-        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(32 * warp) << 16);
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(32 * wq) << 16);
         // every wait's outcome is made uniform over the warp: the tcgen05.st/ld
         // and the shuffles below are warp-collective
         bool ok = __all_sync(0xffffffffu, tc_wait(bar_own, 0, abort));
         // Inputs go in pairs (NI is even): both are split and stored before one
         // tcgen05.wait::st, so a TMEM store round trip is paid once per pair.
-        for (int j0 = 0; j0 < NI && ok; j0 += 2) {
+        for (int j0 = 2 * grp; j0 < NI && ok; j0 += 2 * G) {
             uint32_t pk[2][16];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -474,12 +480,12 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
             for (uint32_t it = 0; it < kTcWait && !tc_try(bar_done, 0); ++it) {
             }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        double acc = 0.0;
+        const bool live = lane_traj < nvalid;
+        const int t = t0 + lane_traj;
+        const float sc = live ? static_cast<float>(sj[t]) : 0.f;
         if (__all_sync(0xffffffffu, done && ok && !*abort)) {
-            const bool live = lane_traj < nvalid;
-            const int t = t0 + lane_traj;
-            const float sc = live ? static_cast<float>(sj[t]) : 0.f;
-            double acc = 0.0;
-            for (int o = 0; o < NQ; ++o) {
+            for (int o = grp; o < NQ; o += G) {
                 uint32_t dv[16];  // [main (8) | correction (8)]
                 tc_ld16(lane_addr + 16 * o, dv);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
@@ -504,12 +510,20 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                     }
                 }
             }
-            if (live) part[static_cast<size_t>(cube) * ldm + t] = acc * static_cast<double>(sc);
         }
+        s_alpha[grp][lane_traj] = acc;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (*abort && tid == 0) atomicOr(status, 4);
+    if (*abort) {
+        if (tid == 0) atomicOr(status, 4);
+    } else if (tid < kTcTraj && tid < nvalid) {
+        // alpha partial of trajectory t0 + tid over this cube, groups in order
+        double a = 0.0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) a += s_alpha[g][tid];
+        part[static_cast<size_t>(cube) * ldm + t0 + tid] = a * static_cast<double>(static_cast<float>(sj[t0 + tid]));
+    }
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::Cols));
