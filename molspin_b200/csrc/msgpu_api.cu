@@ -1028,7 +1028,7 @@ int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
 int tc_tables(msgpu_ctx *c)
 {
     if (!c->tc_ok) return MSGPU_OK;
-    k_tc_tables<<<c->tc_entries, 256, 0, c->stream>>>(static_cast<const int2 *>(c->tc_src.p), c->tc_entries,
+    k_tc_tables<<<c->tc_entries, 128, 0, c->stream>>>(static_cast<const int2 *>(c->tc_src.p), c->tc_entries,
                                                       static_cast<const float4 *>(c->qval.p),
                                                       static_cast<unsigned char *>(c->tc_tab.p));
     const cudaError_t e = cudaGetLastError();

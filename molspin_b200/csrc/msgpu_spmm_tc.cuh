@@ -23,24 +23,27 @@
 //
 // Data path per input quartet (4 rows x 128 trajectories, complex64,
 // pair-planar): TMA bulk copies (one 1 KB row each) into shared memory;
-// 128 producer threads (thread = trajectory = TMEM lane) read their 8 real
-// values (Re/Im of the 4 rows), split each into three BF16 parts
-// x = x0 + x1 + x2 and store [x0 | x1 | x0 | x2] (16 TMEM columns) into a
-// TMEM slot.  Each output quartet owns 16 accumulator columns, [main (8) |
-// correction (8)], and one thread issues, per (output, input) pair, two
-// tcgen05.mma kind::f16 (M = 128 trajectories, N = 16, K = 16, A from TMEM,
-// B from shared memory):
-//     [main | corr] += [x0 | x1] . [[H0 ; H1] | [H1 ; H0]]   (x0 H0 + x1 H1 | x0 H1 + x1 H0)
-//     [main | corr] += [x0 | x2] . [     0    | [H2 ; H0]]   (          0    | x0 H2 + x2 H0)
-// with H = H0 + H1 + H2 the BF16 split of the block's real form (8 x 8:
-// [[Re H, -Im H], [Im H, Re H]] acting on [Re x ; Im x]).  The dropped
-// products are 2^-24 of the result.  The correction products accumulate
-// apart from the main one: the FP32 accumulation of tcgen05.mma rounds
-// towards zero, and keeping the 2^-8-sized corrections out of the main
-// accumulator limits that bias to the main products' own.  An output's first
-// MMA overwrites its 16 columns; the epilogue adds the two halves (round to
-// nearest), scales by s_j, stores U and the per-trajectory FP64 partial of
-// alpha_j = Re <v_j, U>.
+// producer threads (thread = trajectory = TMEM lane; several warpgroups take
+// alternate inputs) read their 8 real values (Re/Im of the 4 rows), split
+// each into a TF32 head and an FP32 tail, x = hi + lo with hi = x with its 13
+// low mantissa bits cleared (exact in TF32) and lo = x - hi (exact in FP32),
+// and store [hi | lo] (16 TMEM columns) into a TMEM slot.  Each output
+// quartet owns 16 accumulator columns, [main (8) | correction (8)], and one
+// thread issues, per (output, input) pair, two tcgen05.mma kind::tf32
+// (M = 128 trajectories, N = 16, K = 8, A from TMEM, B from shared memory):
+//     [main | corr] += hi . [H_hi | H_lo]   (hi H_hi | hi H_lo)
+//     [main | corr] += lo . [  0  | H_hi]   (   0    | lo H_hi)
+// with H = H_hi + H_lo the same split of the block's real form (8 x 8:
+// [[Re H, -Im H], [Im H, Re H]] acting on [Re x ; Im x]).  The dropped lo H_lo
+// and the tensor core's TF32 reading of lo and H_lo are 2^-22 of the result.
+// The correction products accumulate apart from the main one: the FP32
+// accumulation of tcgen05.mma rounds towards zero, and keeping the
+// 2^-11-sized corrections out of the main accumulator limits that bias to the
+// main products' own.  An output's first MMA overwrites its 16 columns; the
+// epilogue adds the two halves (round to nearest), scales by s_j, stores U and
+// the per-trajectory FP64 partial of alpha_j = Re <v_j, U>.  The split costs
+// a producer two instructions per value: the producers, not the tensor pipe,
+// set this kernel's pace.
 //
 // TMEM columns (CB = 4, 512 allocated): accumulators [0, 256), then 16 input
 // slots of 16 columns.  CB = 3 allocates 256 columns (two CTAs per SM).
@@ -50,16 +53,15 @@
 // returns.
 #pragma once
 
-#include <cuda_bf16.h>
-
 #include <cstdint>
+#include <cstring>
 
 #include "msgpu_device.cuh"
 
 namespace msgpu {
 
 constexpr int kTcTraj = 128;            // trajectories per CTA (TMEM lanes, MMA M)
-constexpr int kTcB = 512;               // bytes of one 16 x 16 BF16 B operand
+constexpr int kTcB = 512;               // bytes of one B operand (16 N rows x 8 K TF32)
 constexpr int kTcMaxBits = 14;          // quartet bits P (D <= 65536)
 constexpr uint32_t kTcWait = 1u << 23;  // iterations of a bounded mbarrier wait
 
@@ -131,22 +133,22 @@ __device__ __forceinline__ void tc_arrive(uint32_t bar)
 }
 
 // B operand descriptor: K-major, no swizzle, core matrices of 8 rows x 16 B;
-// LBO = 128 B (the next 8 K), SBO = 256 B (the next 8 N rows), version 1.
+// LBO = 128 B (the next 16 bytes of K), SBO = 256 B (the next 8 N rows), version 1.
 __device__ __forceinline__ uint64_t tc_bdesc(uint32_t addr)
 {
     return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (static_cast<uint64_t>(128 >> 4) << 16) |
            (static_cast<uint64_t>(256 >> 4) << 32) | (static_cast<uint64_t>(1) << 46);
 }
 
-// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major, M = 128, N = 16.
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(16 >> 3) << 17) |
+// kind::tf32 instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 16.
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(16 >> 3) << 17) |
                               (static_cast<uint32_t>(128 >> 4) << 24);
 
 __device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b, uint32_t acc)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}"
         :
         : "r"(d), "r"(a), "l"(b), "r"(kTcIdesc), "r"(acc)
         : "memory");
@@ -176,12 +178,21 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16])
         : "r"(taddr));
 }
 
-// Byte offset of element (n, k) in a 16 x 16 BF16 B operand (see tc_bdesc).
-__host__ __device__ constexpr int tc_boff(int n, int k) { return (n >> 3) * 256 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2; }
+// Byte offset of element (n, k) in a 16 (N) x 8 (K) TF32 B operand (see tc_bdesc).
+__host__ __device__ constexpr int tc_boff(int n, int k) { return (n >> 3) * 256 + (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4; }
 
-__device__ __forceinline__ uint32_t tc_pack(__nv_bfloat16 lo, __nv_bfloat16 hi)
+// TF32 head of x: its 13 low mantissa bits cleared (exact as TF32); x - head is exact in FP32.
+__host__ __device__ inline float tc_head(float x)
 {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+#else
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u &= 0xFFFFE000u;
+    std::memcpy(&x, &u, 4);
+    return x;
+#endif
 }
 
 // Full 4x4 complex block from the compact quartet form (the types of QuartetC).
@@ -224,38 +235,33 @@ __device__ __forceinline__ void tc_expand(int type, const float2 *__restrict__ v
 
 // B-operand tables.  Entry e (src[e] = {value offset in float4 units, type} of
 // a block of the quartet form; offset < 0: no block, a zero operand) becomes
-// two 16 x 16 BF16 B operands of the block's real form R[k][n] (k < 4 Re x_k,
-// 4 <= k < 8 Im x_{k-4}; n < 4 Re y_n, 4 <= n < 8 Im y_{n-4}), with K rows
-// 0..7 against the first operand part and 8..15 against the second:
-//   BA: columns 0..7 [H0; H1] (main), columns 8..15 [H1; H0] (correction)
-//   BB: columns 0..7 zero,            columns 8..15 [H2; H0] (correction)
-// One block of 256 threads per entry, thread (n, k).
-__global__ void __launch_bounds__(256) k_tc_tables(const int2 *__restrict__ src, int nentries,
+// two 16 (N) x 8 (K) TF32 B operands of the block's real form R[k][n] (k < 4
+// Re x_k, 4 <= k < 8 Im x_{k-4}; n < 4 Re y_n, 4 <= n < 8 Im y_{n-4}):
+//   BA: columns 0..7 R_hi (main), columns 8..15 R_lo (correction)
+//   BB: columns 0..7 zero,        columns 8..15 R_hi (correction)
+// One block of 128 threads per entry, thread (n, k).
+__global__ void __launch_bounds__(128) k_tc_tables(const int2 *__restrict__ src, int nentries,
                                                    const float4 *__restrict__ qval, unsigned char *__restrict__ out)
 {
     const int e = blockIdx.x;
     if (e >= nentries) return;
-    const int n = threadIdx.x >> 4, k = threadIdx.x & 15;
+    const int n = threadIdx.x >> 3, k = threadIdx.x & 7;
     const int nn = n & 7;  // the real output component of column n
     float r = 0.f;
     const int2 s = src[e];  // s.x < 0: no such block (zero operand)
     if (s.x >= 0) {
         float2 h[4][4];
         tc_expand(s.y, reinterpret_cast<const float2 *>(qval + s.x), h);
-        const int kk = k & 7, b = kk & 3, a = nn & 3;
+        const int b = k & 3, a = nn & 3;
         const float2 hab = h[a][b];
-        if (kk < 4) r = nn < 4 ? hab.x : hab.y;  // Re x_b -> Re y_a: Re H; -> Im y_a: Im H
-        else r = nn < 4 ? -hab.y : hab.x;        // Im x_b -> Re y_a: -Im H; -> Im y_a: Re H
+        if (k < 4) r = nn < 4 ? hab.x : hab.y;  // Re x_b -> Re y_a: Re H; -> Im y_a: Im H
+        else r = nn < 4 ? -hab.y : hab.x;       // Im x_b -> Re y_a: -Im H; -> Im y_a: Re H
     }
-    const __nv_bfloat16 p0 = __float2bfloat16_rn(r);
-    const float r1 = r - __bfloat162float(p0);
-    const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
-    const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
-    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-    const bool lo = k < 8, main_col = n < 8;
+    const float hi = tc_head(r), lo = r - hi;
+    const bool main_col = n < 8;
     unsigned char *o = out + static_cast<size_t>(e) * 2 * kTcB + tc_boff(n, k);
-    *reinterpret_cast<__nv_bfloat16 *>(o) = main_col ? (lo ? p0 : p1) : (lo ? p1 : p0);  // BA
-    *reinterpret_cast<__nv_bfloat16 *>(o + kTcB) = main_col ? zero : (lo ? p2 : p0);     // BB
+    *reinterpret_cast<float *>(o) = main_col ? hi : lo;            // BA
+    *reinterpret_cast<float *>(o + kTcB) = main_col ? 0.f : hi;    // BB
 }
 
 // U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
@@ -375,12 +381,12 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 const int s = j % NS, r = j / NS;
                 if (!tc_wait(bar_tfull(s), r & 1, abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t a01 = tmem + Cfg::Slot0 + 16 * s, a02 = a01 + 8;
+                const uint32_t a_hi = tmem + Cfg::Slot0 + 16 * s, a_lo = a_hi + 8;
                 const int g = j >> CB, l = j & (NQ - 1);
                 auto issue = [&](int o, uint32_t bt) {
                     const uint32_t d = tmem + 16 * o;
-                    tc_mma(d, a01, tc_bdesc(bt), (written >> o) & 1u);  // the first one overwrites
-                    tc_mma(d, a02, tc_bdesc(bt + kTcB), 1u);
+                    tc_mma(d, a_hi, tc_bdesc(bt), (written >> o) & 1u);  // the first one overwrites
+                    tc_mma(d, a_lo, tc_bdesc(bt + kTcB), 1u);
                     written |= 1u << o;
                 };
                 if (g == 0) {
@@ -438,20 +444,10 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                     if ((tid & 31) == 0) tc_arrive(bar_sempty((j - NQ) % NSTG));
                 }
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    __nv_bfloat16 h0[2], h1[2], h2[2];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const float xv = x[2 * c + e];
-                        h0[e] = __float2bfloat16_rn(xv);
-                        const float r1 = xv - __bfloat162float(h0[e]);
-                        h1[e] = __float2bfloat16_rn(r1);
-                        h2[e] = __float2bfloat16_rn(r1 - __bfloat162float(h1[e]));
-                    }
-                    pk[h][c] = tc_pack(h0[0], h0[1]);
-                    pk[h][4 + c] = tc_pack(h1[0], h1[1]);
-                    pk[h][8 + c] = pk[h][c];
-                    pk[h][12 + c] = tc_pack(h2[0], h2[1]);
+                for (int c = 0; c < 8; ++c) {
+                    const float hi = tc_head(x[c]);
+                    pk[h][c] = __float_as_uint(hi);
+                    pk[h][8 + c] = __float_as_uint(x[c] - hi);
                 }
             }
             if (!ok) break;
