@@ -317,12 +317,13 @@ int msgpu_batch_system_info(const msgpu_batch *batch, int system, int *streamed,
  *   - Problems whose working set does not fit the scratch area are rejected
  *     with MSGPU_ERR_SCRATCH before any work is queued; with krylov_dim 16 the
  *     area holds, e.g., dim 64 with up to 512 trajectories.
+ *   - No call can be captured into a CUDA graph: every call copies its status
+ *     to the host and waits on `stream` (cudaStreamSynchronize) before it
+ *     returns, which a capturing stream refuses (and the capture is lost).
  *   - The first call on a device looks up the scratch address on that device
- *     (cudaGetSymbolAddress); make that first call before any stream capture
- *     starts.  Later calls reuse the address and look it up again only when
- *     it no longer names live device memory (after a cudaDeviceReset).
- *   - Every call copies its status to the host and waits on `stream`
- *     (cudaStreamSynchronize) before it returns.
+ *     (cudaGetSymbolAddress).  Later calls reuse the address and look it up
+ *     again only when it no longer names live device memory (after a
+ *     cudaDeviceReset).
  *   - A CUDA error that is already pending when the call starts is left in
  *     place for the caller and reported as MSGPU_ERR_CUDA; nothing is queued.
  *   - All calls share the one scratch area: calls that may overlap on the GPU

@@ -82,10 +82,13 @@ struct TcCfg {
     static constexpr int OffStage = OffOwn + NQ * InBytes;
     static constexpr int OffDiag = OffStage + NSTG * InBytes;
     static constexpr int OffFlip = OffDiag + NQ * 2 * kTcB;
-    static constexpr int NBar = 2 + 2 * NSTG + 2 * NS + 1;  // own, tables, stage full/empty, slot full/empty, done
+    // own, tables, stage full/empty, slot-quad empty (one commit frees 4 slots), slot full, done
+    static constexpr int NBar = 2 + 2 * NSTG + NS / 4 + NS + 1;
     __host__ __device__ static constexpr int off_bar(int P) { return OffFlip + P * 2 * 2 * kTcB; }
-    __host__ __device__ static constexpr int smem(int P) { return off_bar(P) + NBar * 8 + 16 /*abort, tmem slot*/; }
-    static_assert(NS >= 4, "TMEM slots");
+    // then the abort flag and TMEM slot (16 B) and the first row of every input quartet (int)
+    __host__ __device__ static constexpr int off_rows(int P) { return off_bar(P) + NBar * 8 + 16; }
+    __host__ __device__ static constexpr int smem(int P) { return off_rows(P) + 4 * NQ * (1 + P - CB); }
+    static_assert(NS >= 4 && NS % 4 == 0, "TMEM slots");
 };
 
 __device__ __forceinline__ uint32_t tc_smem(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -267,8 +270,10 @@ __global__ void __launch_bounds__(128) k_tc_tables(const int2 *__restrict__ src,
 // U = s_j H w_j for one trajectory group: grid (Q >> CB cubes, ceil(width / 128)),
 // TcCfg<CB>::Threads threads, TcCfg<CB>::smem(P) bytes of dynamic shared memory.
 //   tflip: [P][2 (output bit)][2] B operands; tdiag: [Q][2] B operands;
-//   quartet_base(q, s1, s2) + {0, s2, s1, s1 + s2}: the rows of quartet q (arithmetic:
-//   the issuing thread must not wait on a load per input);
+//   quartet_base(q, s1, s2) + {0, s2, s1, s1 + s2}: the rows of quartet q (tabled in
+//   shared memory for the CTA's inputs before the roles split);
+//   the MMA issuer frees TMEM input slots four at a time (one tcgen05.commit per quad:
+//   a commit cost the issuer several times an MMA), so NI and NS are multiples of 4;
 //   w, sj, U, part start at the group's first trajectory; width = its
 //   trajectories (a multiple of 64); ldm = the row stride.
 template <int CB>
@@ -290,8 +295,8 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
     auto bar_sfull = [&](int s) { return bar0 + 16 + 8 * s; };
     auto bar_sempty = [&](int s) { return bar0 + 16 + 8 * (NSTG + s); };
     auto bar_tfull = [&](int s) { return bar0 + 16 + 8 * (2 * NSTG + s); };
-    auto bar_tempty = [&](int s) { return bar0 + 16 + 8 * (2 * NSTG + NS + s); };
-    const uint32_t bar_done = bar0 + 16 + 8 * (2 * NSTG + 2 * NS);
+    auto bar_tempty = [&](int s) { return bar0 + 16 + 8 * (2 * NSTG + NS + s / 4); };  // slot s's quad
+    const uint32_t bar_done = bar0 + 16 + 8 * (2 * NSTG + NS + NS / 4);
     volatile int *abort = reinterpret_cast<volatile int *>(sm + Cfg::off_bar(P) + Cfg::NBar * 8);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Cfg::off_bar(P) + Cfg::NBar * 8 + 8);
 
@@ -301,6 +306,16 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
     const int nvalid = min(kTcTraj, width - t0);  // a multiple of 64 (width is)
     const int NI = NQ * (1 + P - CB);             // input quartets
     const int off[4] = {0, s2, s1, s1 + s2};
+    int *rows = reinterpret_cast<int *>(sm + Cfg::off_rows(P));  // first row of input quartet j
+
+    // input j -> quartet (global index): the own cube, then one translated cube per nucleus p >= CB
+    auto input_quartet = [&](int j) {
+        const int g = j >> CB, l = j & (NQ - 1);
+        return g == 0 ? q0 + l : (q0 + l) ^ (1 << (CB + g - 1));
+    };
+    // the row arithmetic (integer divisions) of every input, spread over the CTA:
+    // on the one TMA-issuing thread it took longer than the copies it feeds
+    for (int j = tid; j < NI; j += Cfg::Threads) rows[j] = quartet_base(input_quartet(j), s1, s2);
 
     if (tid == 0) {
         *abort = 0;
@@ -312,7 +327,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
         }
         for (int s = 0; s < NS; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_tfull(s)), "r"(4));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_tempty(s)));
+            if (s % 4 == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_tempty(s)));
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_done));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -327,12 +342,6 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tslot;
 
-    // input j -> quartet (global index): the own cube, then one translated cube per nucleus p >= CB
-    auto input_quartet = [&](int j) {
-        const int g = j >> CB, l = j & (NQ - 1);
-        return g == 0 ? q0 + l : (q0 + l) ^ (1 << (CB + g - 1));
-    };
-
     if (warp == kTmaWarp) {
         // ------------------------------------------------------------ TMA issuer
         if (tid == 32 * kTmaWarp) {
@@ -345,7 +354,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
             // the own cube: NQ quartets x 4 rows, kept for the alpha partial
             tc_expect(bar_own, static_cast<uint32_t>(NQ * 4) * rowbytes);
             for (int l = 0; l < NQ; ++l) {
-                const int b = quartet_base(q0 + l, s1, s2);
+                const int b = rows[l];
                 for (int a = 0; a < 4; ++a)
                     tc_bulk(sbase + Cfg::OffOwn + (l * 4 + a) * kTcTraj * 8, w + static_cast<size_t>(b + off[a]) * ldm + t0,
                             rowbytes, bar_own);
@@ -356,7 +365,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 const int k = j - NQ, s = k % NSTG, r = k / NSTG;
                 if (!tc_wait(bar_sempty(s), (r & 1) ^ 1, abort)) break;
                 tc_expect(bar_sfull(s), 4u * rowbytes);
-                const int b = quartet_base(input_quartet(j), s1, s2);
+                const int b = rows[j];
                 for (int a = 0; a < 4; ++a)
                     tc_bulk(sbase + Cfg::OffStage + s * Cfg::InBytes + a * kTcTraj * 8,
                             w + static_cast<size_t>(b + off[a]) * ldm + t0, rowbytes, bar_sfull(s));
@@ -400,7 +409,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                     const int p = CB + g - 1;
                     issue(l, flip_s + ((p * 2 + ((q0 >> p) & 1)) * 2) * kTcB);
                 }
-                tc_commit(bar_tempty(s));
+                if (s % 4 == 3) tc_commit(bar_tempty(s));  // frees the quad of slots s-3..s
             }
             tc_commit(bar_done);  // completes once every MMA issued above has
         }
@@ -490,7 +499,7 @@ k_lanczos_apply_tc(const unsigned char *__restrict__ tflip, const unsigned char 
                 for (int i = 0; i < 8; ++i) y[i] = (__uint_as_float(dv[8 + i]) + __uint_as_float(dv[i])) * sc;
                 // own input rows of this output (for alpha), pair-planar
                 const unsigned char *own = sm + Cfg::OffOwn + o * Cfg::InBytes;
-                const int b = quartet_base(q0 + o, s1, s2);
+                const int b = rows[o];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const float4 v = *reinterpret_cast<const float4 *>(own + a * kTcTraj * 8 + pair_off);
