@@ -55,6 +55,8 @@ def _args():
                     help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
     ap.add_argument("--combine-tile", type=int, default=0,
                     help="precision form: quartets per CTA of the combine (MSGPU_OPT_COMBINE_TILE; 0 default)")
+    ap.add_argument("--traj-groups", type=int, default=0,
+                    help="precision form: trajectory groups of the step (MSGPU_OPT_TRAJ_GROUPS; 0 default)")
     ap.add_argument("--lanczos-cluster", type=int, default=0,
                     help="precision form: 0 four-kernel Lanczos iteration (default); -1, 1, 2, 4, 8, 16 the "
                          "cluster-resident recurrence (MSGPU_OPT_LANCZOS_CLUSTER)")
@@ -220,6 +222,8 @@ def run_ours(args):
         p.set_option(L.OPT_LANCZOS_CLUSTER, args.lanczos_cluster)
     if args.combine_tile:
         p.set_option(L.OPT_COMBINE_TILE, args.combine_tile)
+    if args.traj_groups:
+        p.set_option(L.OPT_TRAJ_GROUPS, args.traj_groups)
     p.set_hamiltonian(rowptr, col, val)
     p.set_reaction(kappa=sysm.kappa())
     p.set_electron_pair(*sysm.electron_strides())
