@@ -335,6 +335,7 @@ def run_ours(args):
         threads = os.cpu_count() or 1
         cpu = cpu_reference(w, 2 * threads, CPU_SAMPLE_STEPS, threads)
 
+    spmm = p.spmm_choice()  # what the tuner picked (or the forced variant)
     p.close()
     segments = {} if args.no_segments else run_segments(args)
     line = None
@@ -347,7 +348,7 @@ def run_ours(args):
             "config": {"workload": w.name, "trajectories_per_gpu": M, "dim": D, "nnz": int(len(col)),
                        "krylov": w.krylov, "dt_ns": w.dt, "time_steps_per_bench_step": chunk,
                        "l2": "inputs larger than L2 (no flush)", "recurrence": "lanczos", "trajectory_groups": groups,
-                       "parallelism": f"independent trajectory blocks x{world}"},
+                       "spmm": spmm, "parallelism": f"independent trajectory blocks x{world}"},
             "roofline": {"bound": "hbm", "kernel": "quartet SpMM (k_lanczos_apply_*, autotuned variant)", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s", "frac": (achieved / hbm_peak) if achieved else None, "traffic": traffic,
                          "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,

@@ -210,6 +210,13 @@ class HSPropagatorB200:
         _check(self.ctx, L.lib.msgpu_get_option(self.ctx, int(key), C.byref(v)))
         return v.value
 
+    def spmm_choice(self) -> dict:
+        """The quartet SpMM the last complex64 streamed run used: variant, quartet
+        tile and trajectory groups (msgpu_spmm_choice; variant -1 before any run)."""
+        v, t, g = C.c_int(0), C.c_int(0), C.c_int(0)
+        _check(self.ctx, L.lib.msgpu_spmm_choice(self.ctx, C.byref(v), C.byref(t), C.byref(g)))
+        return {"spmm_variant": v.value, "spmm_tile": t.value, "traj_groups": g.value}
+
     def set_form(self, form: str | int):
         """"auto" | "streamed" | "resident" (see MSGPU_FORM_* in include/msgpu.h)."""
         codes = {"auto": L.FORM_AUTO, "streamed": L.FORM_STREAMED, "resident": L.FORM_RESIDENT}

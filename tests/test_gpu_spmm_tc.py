@@ -3,10 +3,10 @@
 against the SIMT quartet SpMM, the complex128 path and the oracle.
 
 Both complex64 SpMMs apply the same FP32 quartet blocks; the tensor-core one
-splits operands into three BF16 parts and accumulates in FP32 in tensor memory
-(dropped products 2^-24 of the result), so yields of the two complex64 forms
-agree to FP32 rounding carried through the run and both stay within the
-precision form's 1e-6 (relative, per trajectory) of complex128.
+splits inputs and blocks into a TF32 head and an FP32 tail and accumulates in
+FP32 in tensor memory (dropped products 2^-22 of the result), so yields of the
+two complex64 forms agree to FP32 rounding carried through the run and both
+stay within the precision form's 1e-6 (relative, per trajectory) of complex128.
 """
 import numpy as np
 import pytest
@@ -42,6 +42,8 @@ def _run(system, F, times, precision, variant=None, noise=None, krylov=16):
         p.profile(True)
         p.propagate(times, krylov, precision)
         napply = p.profile_read(L.KC_APPLY)[1]
+        if variant is not None and precision == "c64":
+            assert p.spmm_choice()["spmm_variant"] == variant  # the forced SpMM is the one that ran
         per, ens = p.yields()
         return per, ens, p.values(), napply
 
