@@ -2036,8 +2036,10 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             for (int j = 0; j < m; ++j) {
                 {
                     Timed tm(c, KC_APPLY);
-                    k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, V,
-                                                               n, j, static_cast<double2 *>(c->part.p), D, ldm, R);
+                    k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, D,
+                                                               ldm, R);
+                    arnoldi_orth_fn(j, 0)<<<grid, kThreads, 0, st>>>(W, V, n, nullptr, static_cast<double2 *>(c->part.p), D,
+                                                                     ldm, R);
                 }
                 {
                     Timed tm(c, KC_REDUCE);
@@ -2046,7 +2048,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_ORTH);
-                    k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h1, static_cast<double2 *>(c->part.p), 1, D, ldm, R);
+                    arnoldi_orth_fn(j, 1)<<<grid, kThreads, 0, st>>>(W, V, n, h1, static_cast<double2 *>(c->part.p), D, ldm, R);
                 }
                 {
                     Timed tm(c, KC_REDUCE);
@@ -2055,7 +2057,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                 }
                 {
                     Timed tm(c, KC_ORTH);
-                    k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h2, static_cast<double2 *>(c->part.p), 2, D, ldm, R);
+                    arnoldi_orth_fn(j, 2)<<<grid, kThreads, 0, st>>>(W, V, n, h2, static_cast<double2 *>(c->part.p), D, ldm, R);
                 }
                 {
                     Timed tm(c, KC_REDUCE);
@@ -2397,12 +2399,12 @@ extern "C" int msgpu_krylov_step_noalloc(int dim, const int *rowptr, const int *
     double2 *W = bufA;
     dim3 grid(nt, ldm / 32);
     for (int j = 0; j < m; ++j) {
-        k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, V, n, j,
-                                                   part, D, ldm, R);
+        k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, D, ldm, R);
+        arnoldi_orth_fn(j, 0)<<<grid, kThreads, 0, st>>>(W, V, n, nullptr, part, D, ldm, R);
         k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(part, nt, j + 1, ldm, h1);
-        k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h1, part, 1, D, ldm, R);
+        arnoldi_orth_fn(j, 1)<<<grid, kThreads, 0, st>>>(W, V, n, h1, part, D, ldm, R);
         k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(part, nt, j + 1, ldm, h2);
-        k_arnoldi_orth<<<grid, kThreads, 0, st>>>(W, V, n, j, h2, part, 2, D, ldm, R);
+        arnoldi_orth_fn(j, 2)<<<grid, kThreads, 0, st>>>(W, V, n, h2, part, D, ldm, R);
         k_reduce_partials<<<dim3(ldm / 32, 1), dim3(32, 8), 0, st>>>(part, nt, 1, ldm, nr);
         k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(h1, h2, nr, j, m, ldm, hess, mdim, sc + ldm);
         src = W;

@@ -17,6 +17,8 @@
 // not depend on how many other trajectories share the launch.
 #pragma once
 
+#include <utility>
+
 #include "msgpu_device.cuh"
 
 namespace msgpu {
@@ -44,26 +46,44 @@ struct CsrF {
 // Arnoldi on G = -iH - K with classical Gram-Schmidt applied twice (CGS2),
 // trajectory tile of 32 (one trajectory per lane, 16-byte loads).
 
-// W = G * v_j where v_j = src * scale[t]; also stores v_j into Vj and writes
-// the first-pass partial dots <V_i, W>, i <= j, to part[tile][i][t].
+// The Krylov index j is a template parameter (J) of k_arnoldi_dots and
+// k_arnoldi_orth, so that the per-trajectory arrays over i <= j (dot
+// accumulators, a row of every V_i) have static indices and live in
+// registers: with a runtime j they sat in local memory, whose traffic spilled
+// to DRAM (more bytes written by the Gram-Schmidt pass than the vector it
+// updates).  The host picks the instantiation from a table
+// (arnoldi_orth_fn); the arithmetic and its order are those of one generic
+// loop over i.
+
+// W = G * v_j where v_j = src * scale[t]; also stores v_j into Vj.  The
+// first-pass dots <V_i, W> are k_arnoldi_dots: fused here they held
+// this kernel (whose CSR gathers want occupancy) to two CTAs per SM.
 __global__ void __launch_bounds__(kThreads)
 k_arnoldi_apply(CsrD H, CsrD K, double kappa, const double2 *__restrict__ src, const double *__restrict__ scale,
-                double2 *__restrict__ Vj, double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride,
-                int j, double2 *__restrict__ part, int D, int ldm, int R)
+                double2 *__restrict__ Vj, double2 *__restrict__ W, int D, int ldm, int R)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = blockIdx.y * 32 + lane;
     const int r0 = blockIdx.x * R;
     const double sc = scale[t];
-    double2 dacc[kMaxKrylov];
-    for (int i = 0; i <= j; ++i) dacc[i] = make_double2(0.0, 0.0);
+    // a row's column indices and values, 32 at a time, staged by the warp with
+    // one coalesced load each, so the gathers below wait on no dependent load
+    __shared__ int scol[kWarps][32];
+    __shared__ double2 sval[kWarps][32];
     for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
         double2 acc = make_double2(0.0, 0.0);
         const int kb = __ldg(H.rowptr + r), ke = __ldg(H.rowptr + r + 1);
-        for (int k = kb; k < ke; ++k) {
-            const int c = __ldg(H.col + k);
-            const double2 h = __ldg(H.val + k);
-            acc = cfma(h, src[static_cast<size_t>(c) * ldm + t], acc);
+        for (int k0 = kb; k0 < ke; k0 += 32) {
+            const int nk = min(32, ke - k0);
+            __syncwarp();
+            if (lane < nk) {
+                scol[warp][lane] = __ldg(H.col + k0 + lane);
+                sval[warp][lane] = __ldg(H.val + k0 + lane);
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int u = 0; u < nk; ++u)
+                acc = cfma(sval[warp][u], src[static_cast<size_t>(scol[warp][u]) * ldm + t], acc);
         }
         acc = cscale(acc, sc);
         const double2 vr = cscale(src[static_cast<size_t>(r) * ldm + t], sc);
@@ -80,62 +100,113 @@ k_arnoldi_apply(CsrD H, CsrD K, double kappa, const double2 *__restrict__ src, c
         const size_t e = static_cast<size_t>(r) * ldm + t;
         Vj[e] = vr;
         W[e] = g;
-        for (int i = 0; i < j; ++i) dacc[i] = cadd(dacc[i], cconjmul(V[i * vstride + e], g));
-        dacc[j] = cadd(dacc[j], cconjmul(vr, g));
+    }
+}
+
+// Partial dots <V_i, W>, i <= j (the first Gram-Schmidt pass; W unchanged,
+// h unused).  Each V_i is used once and the compiler keeps every load of a
+// row in flight; two CTAs per SM bound its registers.
+template <int J>
+__global__ void __launch_bounds__(kThreads, 2)
+k_arnoldi_dots(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride,
+               const double2 *__restrict__ h, double2 *__restrict__ part, int D, int ldm, int R)
+{
+    (void)h;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 32 + lane;
+    const int r0 = blockIdx.x * R;
+    double2 dacc[J + 1];
+#pragma unroll
+    for (int i = 0; i <= J; ++i) dacc[i] = make_double2(0.0, 0.0);
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        const size_t e = static_cast<size_t>(r) * ldm + t;
+        const double2 w = W[e];
+#pragma unroll
+        for (int i = 0; i <= J; ++i) dacc[i] = cadd(dacc[i], cconjmul(__ldg(V + i * vstride + e), w));
     }
     __shared__ double2 sm[kWarps][32];
-    for (int i = 0; i <= j; ++i) {
+#pragma unroll  // static indices keep dacc in registers
+    for (int i = 0; i <= J; ++i) {
         sm[warp][lane] = dacc[i];
         __syncthreads();
         if (warp == 0) {
             double2 s = sm[0][lane];
             for (int w = 1; w < kWarps; ++w) s = cadd(s, sm[w][lane]);
-            part[(static_cast<size_t>(blockIdx.x) * (j + 1) + i) * ldm + t] = s;
+            part[(static_cast<size_t>(blockIdx.x) * (J + 1) + i) * ldm + t] = s;
         }
         __syncthreads();
     }
 }
 
-// W -= sum_{i<=j} h[i][t] V_i ; then partial dots <V_i, W> (mode 1) or the
-// partial squared norm |W|^2 (mode 2, stored in .x).
+// W -= sum_{i<=j} h[i][t] V_i; then partial dots <V_i, W> (MODE 1) or the
+// partial squared norm |W|^2 (MODE 2, stored in .x).  The coefficients sit in
+// shared memory; a row's V_i are all loaded before the first is used.
+template <int J, int MODE>
 __global__ void __launch_bounds__(kThreads)
-k_arnoldi_orth(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride, int j,
-               const double2 *__restrict__ h, double2 *__restrict__ part, int mode, int D, int ldm, int R)
+k_arnoldi_orth(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vstride,
+               const double2 *__restrict__ h, double2 *__restrict__ part, int D, int ldm, int R)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int t = blockIdx.y * 32 + lane;
     const int r0 = blockIdx.x * R;
-    double2 hc[kMaxKrylov];
-    for (int i = 0; i <= j; ++i) hc[i] = h[static_cast<size_t>(i) * ldm + t];
-    double2 dacc[kMaxKrylov];
-    const int nd = mode == 1 ? j + 1 : 1;
-    for (int i = 0; i < nd; ++i) dacc[i] = make_double2(0.0, 0.0);
+    __shared__ double2 hc[J + 1][32];
+    for (int k = threadIdx.x; k < (J + 1) * 32; k += kThreads)
+        hc[k >> 5][k & 31] = h[static_cast<size_t>(k >> 5) * ldm + blockIdx.y * 32 + (k & 31)];
+    __syncthreads();
+    constexpr int ND = MODE == 1 ? J + 1 : 1;
+    double2 dacc[ND];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) dacc[i] = make_double2(0.0, 0.0);
     for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
         const size_t e = static_cast<size_t>(r) * ldm + t;
         double2 w = W[e];
-        double2 vi[kMaxKrylov];
-        for (int i = 0; i <= j; ++i) {
-            vi[i] = V[i * vstride + e];
-            w = csub(w, cmul(hc[i], vi[i]));
-        }
+        double2 vi[J + 1];  // every load of the row in flight before the first use
+#pragma unroll
+        for (int i = 0; i <= J; ++i) vi[i] = __ldg(V + i * vstride + e);
+#pragma unroll
+        for (int i = 0; i <= J; ++i) w = csub(w, cmul(hc[i][lane], vi[i]));
         W[e] = w;
-        if (mode == 1) {
-            for (int i = 0; i <= j; ++i) dacc[i] = cadd(dacc[i], cconjmul(vi[i], w));
+        if (MODE == 1) {
+#pragma unroll
+            for (int i = 0; i <= J; ++i) dacc[i] = cadd(dacc[i], cconjmul(vi[i], w));
         } else {
             dacc[0].x += cabs2(w);
         }
     }
     __shared__ double2 sm[kWarps][32];
-    for (int i = 0; i < nd; ++i) {
+#pragma unroll  // static indices keep dacc in registers
+    for (int i = 0; i < ND; ++i) {
         sm[warp][lane] = dacc[i];
         __syncthreads();
         if (warp == 0) {
             double2 s = sm[0][lane];
             for (int w = 1; w < kWarps; ++w) s = cadd(s, sm[w][lane]);
-            part[(static_cast<size_t>(blockIdx.x) * nd + i) * ldm + t] = s;
+            part[(static_cast<size_t>(blockIdx.x) * ND + i) * ldm + t] = s;
         }
         __syncthreads();
     }
+}
+
+using ArnoldiOrthFn = void (*)(double2 *, const double2 *, size_t, const double2 *, double2 *, int, int, int);
+
+template <int J, int MODE>
+constexpr ArnoldiOrthFn arnoldi_kernel()
+{
+    if constexpr (MODE == 0) return &k_arnoldi_dots<J>;
+    else return &k_arnoldi_orth<J, MODE>;
+}
+template <int MODE, int... J>
+ArnoldiOrthFn arnoldi_orth_pick(int j, std::integer_sequence<int, J...>)
+{
+    static constexpr ArnoldiOrthFn table[] = {arnoldi_kernel<J, MODE>()...};
+    return table[j];
+}
+// The kernel of iteration j, 0 <= j < kMaxKrylov: mode 0 k_arnoldi_dots,
+// modes 1 and 2 k_arnoldi_orth.
+inline ArnoldiOrthFn arnoldi_orth_fn(int j, int mode)
+{
+    constexpr auto js = std::make_integer_sequence<int, kMaxKrylov>{};
+    return mode == 0 ? arnoldi_orth_pick<0>(j, js) : mode == 1 ? arnoldi_orth_pick<1>(j, js) : arnoldi_orth_pick<2>(j, js);
 }
 
 // out[i][t] = sum over tiles of part[tile][i][t] (fixed order).
