@@ -181,9 +181,19 @@ int msgpu_set_hamiltonian_coefficients(msgpu_ctx *ctx, const double *coef);
  * coefficients, row j for global step first_step + j, evaluated by the caller
  * at that step's midpoint; each step of msgpu_run then propagates with
  * sum_k coef_k H_k, combined on the device.  Streamed Krylov and Taylor
- * propagators; the dense propagator and the resident form need a static H.
+ * propagators (RK4 takes msgpu_set_hamiltonian_schedule_rk4); the dense
+ * propagator and the resident form need a static H.
  * nsteps = 0 clears the schedule. */
 int msgpu_set_hamiltonian_schedule(msgpu_ctx *ctx, const double *coef, long long first_step, long long nsteps);
+/* Time-dependent H for the RK4 propagator (HSPropagator::StepDynamicRK4,
+ * HSPropagator.cpp:104-128, and StepDynamicRK4Stochastic, :142-150): RK4 on
+ * dB/dt = G(t) B needs G at the start, midpoint and end of each step.  coef
+ * holds 2 nsteps + 1 rows of nterms coefficients: row 2j at the start of
+ * global step first_step + j, row 2j + 1 at its midpoint, row 2j + 2 at its
+ * end (the next step's start).  The Krylov and Taylor propagators use the
+ * midpoint rows of the same schedule.  K stays time-independent.  nsteps = 0
+ * clears the schedule. */
+int msgpu_set_hamiltonian_schedule_rk4(msgpu_ctx *ctx, const double *coef, long long first_step, long long nsteps);
 
 /* K = kappa * I (symmetric recombination: kappa = k/2,
  * HSReactionRelaxation::BuildReactionForOrientation, HSReactionRelaxation.cpp:134-164). */

@@ -86,6 +86,7 @@ def _load() -> C.CDLL:
         "msgpu_upload_hamiltonian_terms": (I, [P, I, pI, pI, I, pD, pD]),
         "msgpu_set_hamiltonian_coefficients": (I, [P, pD]),
         "msgpu_set_hamiltonian_schedule": (I, [P, pD, C.c_longlong, C.c_longlong]),
+        "msgpu_set_hamiltonian_schedule_rk4": (I, [P, pD, C.c_longlong, C.c_longlong]),
         "msgpu_set_reaction_scalar": (I, [P, D]),
         "msgpu_upload_reaction_csr": (I, [P, pI, pI, pD]),
         "msgpu_set_electron_pair": (I, [P, I, I]),

@@ -78,10 +78,13 @@ struct msgpu_ctx {
     DevBuf hterms, qsrc;   // nterms x nnz complex128; CSR index of every quartet value slot (-1: zero)
     size_t q_nslots = 0;
     std::array<double, 16> hcoef{};  // current coefficients
-    // time-dependent H: coefficients per global step (sched_steps x nterms),
-    // evaluated by the caller at each step's midpoint
+    // time-dependent H: coefficients per global step, evaluated by the caller
+    // at each step's midpoint (sched_rows = 1: sched_steps x nterms) or at its
+    // start and midpoint plus the last step's end (sched_rows = 2, the
+    // dynamic RK4 layout: (2 sched_steps + 1) x nterms)
     std::vector<double> sched;
     long long sched_first = 0, sched_steps = 0;
+    int sched_rows = 1;
     // tensor-core SpMM (k_lanczos_apply_tc): B-operand tables of the quartet
     // form, built when the quartet form has the nuclear-bit structure
     DevBuf tc_src, tc_tab;
@@ -1706,23 +1709,51 @@ int msgpu_set_hamiltonian_coefficients(msgpu_ctx *c, const double *coef)
     return MSGPU_OK;
 }
 
-int msgpu_set_hamiltonian_schedule(msgpu_ctx *c, const double *coef, long long first_step, long long nsteps)
+namespace {
+
+// rows_per_step 1: one midpoint row per step; 2: start and midpoint rows per
+// step plus one final end row (row 2j + 2 is step j's end and step j+1's start)
+int set_schedule(msgpu_ctx *c, const double *coef, long long first_step, long long nsteps, int rows_per_step)
 {
     if (!c) return MSGPU_ERR_INVALID;
     if (nsteps == 0) {
         c->sched.clear();
         c->sched_steps = 0;
+        c->sched_rows = 1;
         return MSGPU_OK;
     }
     if (!c->terms) return fail(c, MSGPU_ERR_STATE, "Hamiltonian schedule: no terms uploaded");
     if (!coef || nsteps < 0 || first_step < 0) return fail(c, MSGPU_ERR_INVALID, "Hamiltonian schedule: invalid arguments");
-    const size_t n = static_cast<size_t>(nsteps) * c->nterms;
+    const size_t rows = rows_per_step == 1 ? static_cast<size_t>(nsteps) : 2 * static_cast<size_t>(nsteps) + 1;
+    const size_t n = rows * c->nterms;
     for (size_t i = 0; i < n; ++i)
         if (!std::isfinite(coef[i])) return fail(c, MSGPU_ERR_NONFINITE, "Hamiltonian schedule: non-finite coefficient");
     c->sched.assign(coef, coef + n);
     c->sched_first = first_step;
     c->sched_steps = nsteps;
+    c->sched_rows = rows_per_step;
     return MSGPU_OK;
+}
+
+// Coefficient row of global step g at point which (0 start, 1 midpoint, 2 end);
+// a midpoint-only schedule has only which = 1.
+const double *sched_row(const msgpu_ctx *c, long long g, int which)
+{
+    const size_t k = static_cast<size_t>(g - c->sched_first);
+    const size_t row = c->sched_rows == 1 ? k : 2 * k + static_cast<size_t>(which);
+    return c->sched.data() + row * c->nterms;
+}
+
+}  // namespace
+
+int msgpu_set_hamiltonian_schedule(msgpu_ctx *c, const double *coef, long long first_step, long long nsteps)
+{
+    return set_schedule(c, coef, first_step, nsteps, 1);
+}
+
+int msgpu_set_hamiltonian_schedule_rk4(msgpu_ctx *c, const double *coef, long long first_step, long long nsteps)
+{
+    return set_schedule(c, coef, first_step, nsteps, 2);
 }
 
 int msgpu_upload_factors(msgpu_ctx *c, int dim, int ntraj, const double *factors)
@@ -1795,8 +1826,10 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     if (p->propagator != MSGPU_PROP_KRYLOV && !taylor && !rk4) return fail(c, MSGPU_ERR_INVALID, "run: unknown propagator");
     if ((taylor || rk4) && p->precision != MSGPU_PREC_C128)
         return fail(c, MSGPU_ERR_INVALID, "run: the Taylor and RK4 propagators are complex128 only");
-    if (rk4 && c->sched_steps)
-        return fail(c, MSGPU_ERR_INVALID, "run: the RK4 propagator takes a time-independent H (dynamic RK4 is not built)");
+    if (rk4 && c->sched_steps && c->sched_rows != 2)
+        return fail(c, MSGPU_ERR_INVALID,
+                    "run: RK4 with a time-dependent H needs the start, midpoint and end coefficients of every step "
+                    "(msgpu_set_hamiltonian_schedule_rk4)");
     if (!taylor && !rk4 && (p->krylov_dim < 1 || p->krylov_dim > kMaxKrylov))
         return fail(c, MSGPU_ERR_INVALID, "run: krylov_dim must be in 1..32");
     int rec = p->recurrence;
@@ -1950,10 +1983,10 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         c->prof_tick = s;
         const double dt = p->times[s + 1] - p->times[s];
         const long long g = g0 + s;
-        if (c->sched_steps) {
+        if (c->sched_steps && !rk4) {
             // H at this step's midpoint from the schedule: combine the terms
             // on the device, refresh the quartet values of the complex64 form
-            const double *row = c->sched.data() + static_cast<size_t>(g - c->sched_first) * c->nterms;
+            const double *row = sched_row(c, g, 1);
             TermCoef cf;
             std::memset(&cf, 0, sizeof(cf));
             double hs[3] = {0.0, 0.0, 0.0};
@@ -2014,6 +2047,19 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             const double2 *in[4] = {psi, ya, yb, ya};
             double2 *out[4] = {ya, yb, ya, nullptr};
             for (int stage = 0; stage < 4; ++stage) {
+                if (c->sched_steps && stage != 2) {
+                    // dynamic RK4 (HSPropagator.cpp:104-128): G at the step's start
+                    // (stage 1), midpoint (stages 2, 3) and end (stage 4); the
+                    // stages are stream-ordered, so H is recombined in place
+                    const double *row = sched_row(c, g, stage == 0 ? 0 : stage == 1 ? 1 : 2);
+                    TermCoef cf;
+                    std::memset(&cf, 0, sizeof(cf));
+                    for (int k = 0; k < c->nterms; ++k) cf.c[k] = row[k];
+                    k_combine_terms<<<ceil_div(std::max(1, c->nnz), 256), 256, 0, st>>>(
+                        static_cast<const double2 *>(c->hterms.p), c->nterms, cf, c->nnz,
+                        static_cast<double2 *>(c->hval.p), static_cast<float2 *>(c->hhi.p),
+                        static_cast<float2 *>(c->hlo.p), static_cast<int *>(c->status.p));
+                }
                 Timed tm(c, KC_APPLY);
                 k_rk4_stage<<<tgrid, tblock, 0, st>>>(Hd, Kd, kappa, in[stage], psi, out[stage], acc, cs[stage],
                                                       ws[stage], stage + 1, D, ldm);

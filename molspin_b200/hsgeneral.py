@@ -137,6 +137,19 @@ class HSPropagatorB200:
         _check(self.ctx, L.lib.msgpu_set_hamiltonian_schedule(self.ctx, L.dptr(c.reshape(-1)), int(first_step),
                                                               int(c.shape[0])))
 
+    def set_hamiltonian_schedule_rk4(self, coef, first_step: int = 0):
+        """coef: (2 nsteps + 1, nterms) coefficients for the RK4 propagator with a
+        time-dependent H: row 2j at the start of global step first_step + j, row
+        2j + 1 at its midpoint, row 2j + 2 at its end; None clears the schedule."""
+        if coef is None:
+            _check(self.ctx, L.lib.msgpu_set_hamiltonian_schedule_rk4(self.ctx, None, 0, 0))
+            return
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        if c.shape[0] < 3 or c.shape[0] % 2 != 1:
+            raise ValueError("an RK4 schedule has 2 nsteps + 1 rows")
+        _check(self.ctx, L.lib.msgpu_set_hamiltonian_schedule_rk4(self.ctx, L.dptr(c.reshape(-1)), int(first_step),
+                                                                  int((c.shape[0] - 1) // 2)))
+
     def set_reaction(self, kappa: float | None = None, csr=None):
         if csr is None:
             _check(self.ctx, L.lib.msgpu_set_reaction_scalar(self.ctx, float(kappa)))

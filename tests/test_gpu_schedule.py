@@ -112,3 +112,68 @@ def test_schedule_against_stepwise_oracle(propagator):
     ref_values.append(out["values"][1])
     ref_values = np.asarray(ref_values)
     assert np.max(np.abs(values - ref_values)) < 1e-10 * np.max(np.abs(ref_values))
+
+
+def _rk4_rows(times):
+    """Coefficient rows of an RK4 schedule: each step's start and midpoint, then the last end."""
+    rows = []
+    for k in range(len(times) - 1):
+        rows.append([1.0, *_field(times[k])])
+        rows.append([1.0, *_field(0.5 * (times[k] + times[k + 1]))])
+    rows.append([1.0, *_field(times[-1])])
+    return np.array(rows)
+
+
+def test_dynamic_rk4_against_oracle():
+    # RK4 with G at each step's start, midpoint and end (StepDynamicRK4Stochastic)
+    # against the numpy restatement, replayed noise: within 1e-10
+    import scipy.sparse as sp
+    from oracle import dynamic as dyn
+    s = _system()
+    r, c, v = S.field_terms(s)
+    D, M = s.dim, 16
+    times = S.time_grid(12.0, 0.5)
+    F = s.trace_samples(M, 5.0)
+    rng = np.random.default_rng(21)
+    bits = np.packbits(rng.integers(0, 2, size=2 * (len(times) - 1) * M).astype(np.uint8), bitorder="little")
+    with hs.HSPropagatorB200(0) as p:
+        _ctx(p, s, F, r, c, v, (s.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
+        p.set_hamiltonian_schedule_rk4(_rk4_rows(times))
+        p.propagate(times, 12, "c128", propagator="rk4")
+        values = p.values()
+    terms = [sp.csr_matrix((v[k], c, r), shape=(D, D)).toarray() for k in range(v.shape[0])]
+
+    def H_at(t):
+        return sum(ck * T for ck, T in zip([1.0, *_field(t)], terms))
+
+    obs = [(sp.csr_matrix((o[0][2], o[0][1], o[0][0]), shape=(D, D)).toarray(), o[1]) for o in h.oracle_observables(s)]
+    ur, uc, uv = orc.st_unitary(s.mult, *s.electrons)
+    U = sp.csr_matrix((uv, uc, ur), shape=(D, D)).toarray()
+    ref = dyn.dynamic_rk4_stochastic(H_at, s.kappa(), F, times, obs, U, bits)
+    assert np.max(np.abs(values - ref)) < 1e-10 * np.max(np.abs(ref))
+
+
+def test_rk4_schedule_midpoints_drive_krylov_and_rk4_needs_them():
+    # the Krylov step reads the midpoint rows of an RK4 schedule: bitwise the
+    # run with the midpoint schedule; RK4 with a midpoint-only schedule is refused
+    s = _system()
+    r, c, v = S.field_terms(s)
+    M, times = 16, S.time_grid(8.0, 1.0)
+    F = s.trace_samples(M, 7.0)
+    mids = 0.5 * (times[1:] + times[:-1])
+    noise = (s.st_rate, L.NOISE_PHILOX, 13)
+    out = []
+    for rk in (False, True):
+        with hs.HSPropagatorB200(0) as p:
+            _ctx(p, s, F, r, c, v, noise)
+            if rk:
+                p.set_hamiltonian_schedule_rk4(_rk4_rows(times))
+            else:
+                p.set_hamiltonian_schedule(np.array([[1.0, *_field(t)] for t in mids]))
+            p.propagate(times, 12, "c128")
+            out.append(p.values())
+            if not rk:
+                with pytest.raises(hs.MsgpuError) as e:
+                    p.propagate(times, 12, "c128", propagator="rk4")
+                assert e.value.code == L.MSGPU_ERR_INVALID
+    np.testing.assert_array_equal(out[0], out[1])

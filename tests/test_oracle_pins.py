@@ -260,3 +260,32 @@ def test_trace_sampling_structure():
     rho = F @ F.conj().T
     target = np.kron(S.pair_projector(S.SINGLET), np.eye(2) / 2)
     assert np.linalg.norm(rho - target) < 6 / math.sqrt(M)
+
+
+def _dense(csr, D):
+    import scipy.sparse as sp
+    r, c, v = csr
+    return sp.csr_matrix((v, c, r), shape=(D, D)).toarray()
+
+
+def test_dynamic_rk4_oracle_reduces_to_the_c_oracle_rk4():
+    # The numpy restatement of StepDynamicRK4Stochastic (oracle/dynamic.py)
+    # with a constant H is the C oracle's RK4 loop (method 2) with the same
+    # replayed noise bits: pins the restatement's stage order, noise halves
+    # and evaluation points.
+    from oracle import dynamic as dyn
+    s = h.random_system([2, 2], [2], seed=5, aniso=True, st_rate=0.2)  # D = 32
+    D, M = s.dim, 6
+    times = S.time_grid(12.0, 0.5)
+    F = s.trace_samples(M, 3.0)
+    rng = np.random.default_rng(11)
+    bits = np.packbits(rng.integers(0, 2, size=2 * (len(times) - 1) * M).astype(np.uint8), bitorder="little")
+    Hc = s.hamiltonian_csr()
+    Ucsr = orc.st_unitary(s.mult, *s.electrons)
+    obs = h.oracle_observables(s)
+    ref = orc.hs_stochastic(Hc, F, times, obs, kappa=s.kappa(), method=2, U_csr=Ucsr, event_rate=0.5 * s.st_rate,
+                            noise_mode=1, flip_bits=bits)
+    Hd = _dense(Hc, D)
+    got = dyn.dynamic_rk4_stochastic(lambda t: Hd, s.kappa(), F, times, [(_dense(o, D), r) for o, r in obs],
+                                     _dense(Ucsr, D), bits)
+    assert np.max(np.abs(got - ref["values"])) < 1e-12 * np.max(np.abs(ref["values"]))
