@@ -217,7 +217,14 @@ int msgpu_add_pair_observable(msgpu_ctx *ctx, const double *op4x4, double rate);
  * unitary U = PS - PT is applied with per-half-step probability
  * -expm1(-st_rate*h)/2 (SpinSpace_relaxation.cpp:1233).  For
  * MSGPU_NOISE_REPLAY, bits holds one bit per (step, half, trajectory) at
- * index (step*2 + half)*ntraj + t for nsteps steps. */
+ * index (step*2 + half)*ntraj + t for nsteps steps.  Several dephasing
+ * Operators on the same pair: st_rate = the sum of their rates.  Every
+ * channel applies P_S - P_T, so the superposed-Poisson branch
+ * (SpinSpace_relaxation.cpp:1239-1252) acts through the parity of its event
+ * count alone, and the odd-parity probability at the summed rate is the
+ * one-channel formula: MSGPU_NOISE_PHILOX then draws it on the device, and
+ * msgpu_host_reference_flip_bits_multi gives the reference's own bits for
+ * MSGPU_NOISE_REPLAY. */
 int msgpu_set_st_noise(msgpu_ctx *ctx, double st_rate, int mode, unsigned long long seed,
                        const unsigned char *bits, long long nsteps, int ntraj);
 

@@ -251,6 +251,33 @@ def test_multi_term_dephasing_stream_replayed():
     per, ens, _, _ = _gpu(system, F, times, 16, noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
     ref = _oracle(system, F, times, 16, U=True, kappa=system.kappa(), noise_mode=1, flip_bits=bits)
     assert _rel(per, ref["traj_yield"]) < 1e-10
+    # the complex64 form (streamed Lanczos) replays the same parity bits
+    per64, _, _, _ = _gpu(system, F, times, 16, precision="c64", form="streamed",
+                          noise=(system.st_rate, L.NOISE_REPLAY, 0, bits, len(times) - 1, M))
+    assert _rel(per64, ref["traj_yield"]) < 1e-6
+
+
+def test_multi_term_dephasing_philox_is_the_summed_rate():
+    # Every channel applies P_S - P_T, so only the parity of the superposed
+    # Poisson count acts; its odd probability is the one-channel formula at
+    # the summed rate.  The device's Philox stream at the summed rate against
+    # the exact density-matrix yield (the Lindblad sum of the channels), both
+    # precisions, within 5 standard errors of the trajectory mean.
+    system = h.random_system([2, 2], [2], seed=14, st_rate=0.0, hf_scale=2.0)  # D = 32
+    rates = [0.2, 0.3]
+    system.st_rate = sum(rates)
+    M, times = 4096, S.time_grid(20.0, 0.5)
+    F = system.trace_samples(M, 5.0)
+    H = den.dense_hamiltonian(system)
+    K = system.kappa() * np.eye(system.dim)
+    ops = [(den.pair_operator(op, system), rate) for _, op, rate in system.observables()]
+    _, ref = den.propagate_density(H, K, den.singlet_density(system), times, ops, U=den.st_unitary(system),
+                                   st_rate=system.st_rate)
+    for precision in ("c128", "c64"):
+        per, ens, _, _ = _gpu(system, F, times, 16, precision=precision, form="streamed",
+                              noise=(system.st_rate, L.NOISE_PHILOX, 41))
+        se = np.std(per, axis=0) * np.sqrt(M)
+        assert np.all(np.abs(ens - ref) < 5 * se + 1e-12), (precision, ens, ref, se)
 
 
 @pytest.mark.parametrize("variant", [4, 5, 6, 7])
