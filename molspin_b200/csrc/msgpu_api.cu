@@ -52,6 +52,7 @@ struct msgpu_ctx {
     std::vector<double> h_val;
     // quartet-block form of H for the current electron strides
     DevBuf qrow, qcolt, qval, qbase;
+    DevBuf qval64;  // the quartet values in FP64 (complex128 Arnoldi apply)
     int q_s1 = 0, q_s2 = 0, q_D = 0, q_nblocks = 0;
     long long q_build = 0;            // counts quartet-form builds
     std::vector<int> q_hrow;          // host copies of the quartet form
@@ -320,7 +321,7 @@ void msgpu_destroy(msgpu_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     collect_profile(c);
-    DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->qrow, &c->qcolt, &c->qval, &c->qbase,
+    DevBuf *all[] = {&c->hrow, &c->hcol, &c->hval, &c->hhi, &c->hlo, &c->qrow, &c->qcolt, &c->qval, &c->qbase, &c->qval64,
                      &c->fblk, &c->fval, &c->frow, &c->fdsrc, &c->fdiag, &c->krow, &c->kcol, &c->kval, &c->bits,
                      &c->psi128, &c->basis, &c->wbuf, &c->zbuf, &c->ubuf, &c->part, &c->part2, &c->hess,
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
@@ -623,15 +624,17 @@ __global__ void k_combine_terms(const double2 *__restrict__ terms, int nterms, T
                         static_cast<float>(v.y - static_cast<double>(h.y)));
 }
 
-// quartet value slot s (two FP32 per complex value) <- the CSR value it came from
+// quartet value slot s (two FP32 per complex value, and its FP64 copy) <- the
+// CSR value it came from
 __global__ void k_quartet_refresh(const int *__restrict__ src, size_t nslots, const double2 *__restrict__ val,
-                                  float2 *__restrict__ qval)
+                                  float2 *__restrict__ qval, double2 *__restrict__ qval64)
 {
     const size_t s = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (s >= nslots) return;
     const int k = src[s];
     const double2 v = k >= 0 ? val[k] : make_double2(0.0, 0.0);
     qval[s] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    qval64[s] = v;
 }
 
 }  // namespace
@@ -1043,7 +1046,7 @@ int refresh_quartet_values(msgpu_ctx *c)
     if (!c->q_nslots) return MSGPU_OK;
     k_quartet_refresh<<<static_cast<unsigned>((c->q_nslots + 255) / 256), 256, 0, c->stream>>>(
         static_cast<const int *>(c->qsrc.p), c->q_nslots, static_cast<const double2 *>(c->hval.p),
-        static_cast<float2 *>(c->qval.p));
+        static_cast<float2 *>(c->qval.p), static_cast<double2 *>(c->qval64.p));
     const cudaError_t e = cudaGetLastError();
     if (e) return cuda_fail(c, e, "quartet value refresh");
     return c->tc_build == c->q_build ? tc_tables(c) : MSGPU_OK;
@@ -1057,6 +1060,7 @@ int build_quartet(msgpu_ctx *c)
     std::vector<int> rowptr(Q + 1, 0), base(Q);
     std::vector<int2> blks;
     std::vector<float> vals;
+    std::vector<double> vals64;  // the same values in FP64
     std::vector<std::pair<int, std::array<double, 32>>> blocks;  // (neighbour base, 16 complex)
     std::vector<std::array<int, 16>> bsrc;                        // CSR index of each block entry
     std::vector<int> src;                                         // CSR index per stored value slot
@@ -1141,6 +1145,8 @@ int build_quartet(msgpu_ctx *c)
             for (auto &ab : order) {
                 vals.push_back(static_cast<float>(re(ab.first, ab.second)));
                 vals.push_back(static_cast<float>(im(ab.first, ab.second)));
+                vals64.push_back(re(ab.first, ab.second));
+                vals64.push_back(im(ab.first, ab.second));
                 src.push_back(bsrc[oi][ab.first * 4 + ab.second]);
             }
         }
@@ -1151,12 +1157,15 @@ int build_quartet(msgpu_ctx *c)
     if ((rc = ensure(c, c->qrow, sizeof(int) * (Q + 1), "quartet rowptr")) ||
         (rc = ensure(c, c->qcolt, sizeof(int2) * std::max(1, nb), "quartet blocks")) ||
         (rc = ensure(c, c->qval, sizeof(float) * std::max<size_t>(4, vals.size()), "quartet values")) ||
+        (rc = ensure(c, c->qval64, sizeof(double) * std::max<size_t>(4, vals64.size()), "quartet values (FP64)")) ||
         (rc = ensure(c, c->qbase, sizeof(int) * Q, "quartet bases")))
         return rc;
     cudaError_t e;
     if ((e = cudaMemcpyAsync(c->qrow.p, rowptr.data(), sizeof(int) * (Q + 1), cudaMemcpyHostToDevice, c->stream)) ||
         (e = cudaMemcpyAsync(c->qcolt.p, blks.data(), sizeof(int2) * nb, cudaMemcpyHostToDevice, c->stream)) ||
         (e = cudaMemcpyAsync(c->qval.p, vals.data(), sizeof(float) * vals.size(), cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(c->qval64.p, vals64.data(), sizeof(double) * vals64.size(), cudaMemcpyHostToDevice,
+                             c->stream)) ||
         (e = cudaMemcpyAsync(c->qbase.p, base.data(), sizeof(int) * Q, cudaMemcpyHostToDevice, c->stream)) ||
         (e = cudaStreamSynchronize(c->stream)))
         return cuda_fail(c, e, "quartet upload");
@@ -1926,6 +1935,10 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     }
     yield_update(0.0, 1, 0);
     int fused_c = 0;  // cluster size of k_lanczos_fused, 0: the four-kernel iteration
+    // the complex128 Arnoldi apply runs over quartet blocks when K = kappa I
+    const bool quartet128 = prec == MSGPU_PREC_C128 && !taylor && !rk4 && c->k_scalar;
+    if (quartet128)
+        if (int rc = build_quartet(c)) return rc;
     if (prec == MSGPU_PREC_C64) {
         if (int rc = build_quartet(c)) return rc;
         if (int rc = build_tc(c)) return rc;
@@ -2001,7 +2014,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             k_combine_terms<<<ceil_div(std::max(1, c->nnz), 256), 256, 0, st>>>(
                 static_cast<const double2 *>(c->hterms.p), c->nterms, cf, c->nnz, static_cast<double2 *>(c->hval.p),
                 static_cast<float2 *>(c->hhi.p), static_cast<float2 *>(c->hlo.p), static_cast<int *>(c->status.p));
-            if (prec == MSGPU_PREC_C64)
+            if (prec == MSGPU_PREC_C64 || quartet128)
                 if (int rc = refresh_quartet_values(c)) return rc;
             if (taylor) taylor_shift(hs);
         }
@@ -2082,8 +2095,14 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             for (int j = 0; j < m; ++j) {
                 {
                     Timed tm(c, KC_APPLY);
-                    k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, D,
-                                                               ldm, R);
+                    if (quartet128)
+                        k_arnoldi_apply_q<<<dim3(ceil_div(Q, kWarps), ldm / 32), kThreads, 0, st>>>(
+                            QuartetD{static_cast<const int *>(c->qrow.p), static_cast<const int2 *>(c->qcolt.p),
+                                     static_cast<const double2 *>(c->qval64.p), static_cast<const int *>(c->qbase.p)},
+                            kappa, src, j == 0 ? sc : sc + ldm, V + j * n, W, Q, c->s1, c->s2, ldm);
+                    else
+                        k_arnoldi_apply<<<grid, kThreads, 0, st>>>(Hd, Kd, kappa, src, j == 0 ? sc : sc + ldm, V + j * n,
+                                                                   W, D, ldm, R);
                     arnoldi_orth_fn(j, 0)<<<grid, kThreads, 0, st>>>(W, V, n, nullptr, static_cast<double2 *>(c->part.p), D,
                                                                      ldm, R);
                 }

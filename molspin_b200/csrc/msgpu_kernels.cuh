@@ -103,6 +103,114 @@ k_arnoldi_apply(CsrD H, CsrD K, double kappa, const double2 *__restrict__ src, c
     }
 }
 
+// The complex128 quartet form: the compact blocks of QuartetC with FP64
+// values (double2 per complex value, in the same order; a block's value
+// offset counts float4 units, two complex values each).
+struct QuartetD {
+    const int *rowptr;   // Q + 1
+    const int2 *blk;     // nblocks
+    const double2 *val;  // complex values
+    const int *base;     // Q
+};
+
+// o[a] += sum_b B[a][b] x[b] for one compact block of type `type` (the
+// layouts of QuartetC), complex128.
+__device__ __forceinline__ void quartet_block_d(double2 o[4], int type, const double2 *__restrict__ v,
+                                                const double2 x[4])
+{
+    switch (type) {
+    case 0:
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) o[a] = cfma(__ldg(v + 4 * a + b), x[b], o[a]);
+        break;
+    case 1:  // [a2][a1][b1]
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2)
+#pragma unroll
+            for (int a1 = 0; a1 < 2; ++a1)
+#pragma unroll
+                for (int b1 = 0; b1 < 2; ++b1)
+                    o[2 * a1 + a2] = cfma(__ldg(v + (2 * a2 + a1) * 2 + b1), x[2 * b1 + a2], o[2 * a1 + a2]);
+        break;
+    case 2:  // [a1][a2][b2]
+#pragma unroll
+        for (int a1 = 0; a1 < 2; ++a1)
+#pragma unroll
+            for (int a2 = 0; a2 < 2; ++a2)
+#pragma unroll
+                for (int b2 = 0; b2 < 2; ++b2)
+                    o[2 * a1 + a2] = cfma(__ldg(v + (2 * a1 + a2) * 2 + b2), x[2 * a1 + b2], o[2 * a1 + a2]);
+        break;
+    case 3:
+#pragma unroll
+        for (int a = 0; a < 4; ++a) o[a] = cfma(__ldg(v + a), x[a], o[a]);
+        break;
+    case 4: {  // A (x) I on digit 1: [a1][b1]
+        const double2 A00 = __ldg(v), A01 = __ldg(v + 1), A10 = __ldg(v + 2), A11 = __ldg(v + 3);
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+            const double2 x0 = x[a2], x1 = x[2 + a2];
+            o[a2] = cfma(A01, x1, cfma(A00, x0, o[a2]));
+            o[2 + a2] = cfma(A11, x1, cfma(A10, x0, o[2 + a2]));
+        }
+        break;
+    }
+    default: {  // I (x) A on digit 2: [a2][b2]
+        const double2 A00 = __ldg(v), A01 = __ldg(v + 1), A10 = __ldg(v + 2), A11 = __ldg(v + 3);
+#pragma unroll
+        for (int a1 = 0; a1 < 2; ++a1) {
+            const double2 x0 = x[2 * a1], x1 = x[2 * a1 + 1];
+            o[2 * a1] = cfma(A01, x1, cfma(A00, x0, o[2 * a1]));
+            o[2 * a1 + 1] = cfma(A11, x1, cfma(A10, x0, o[2 * a1 + 1]));
+        }
+        break;
+    }
+    }
+}
+
+// k_arnoldi_apply over quartet blocks for K = kappa I: a warp per output
+// quartet, a lane per trajectory.  A row and trajectory gathers 13 quartet
+// rows of 16 B at D = 16384 (radical pair, 12 nuclear spins) against 27 CSR
+// entries, and the block descriptors and values are loaded once per quartet
+// for its four rows.  Summation runs in block order, not CSR order.
+__global__ void __launch_bounds__(kThreads)
+k_arnoldi_apply_q(QuartetD H, double kappa, const double2 *__restrict__ src, const double *__restrict__ scale,
+                  double2 *__restrict__ Vj, double2 *__restrict__ W, int Q, int s1, int s2, int ldm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 32 + lane;
+    const int q = blockIdx.x * kWarps + warp;
+    if (q >= Q) return;
+    const double sc = scale[t];
+    const int off[4] = {0, s2, s1, s1 + s2};
+    double2 o[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) o[a] = make_double2(0.0, 0.0);
+    double2 x[4];
+    int last = -1;
+    const int kb = __ldg(H.rowptr + q), ke = __ldg(H.rowptr + q + 1);
+    for (int kk = kb; kk < ke; ++kk) {
+        const int2 cur = __ldg(H.blk + kk);
+        last = cur.x >> 3;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) x[b] = src[static_cast<size_t>(last + off[b]) * ldm + t];
+        quartet_block_d(o, cur.x & 7, H.val + 2 * static_cast<size_t>(cur.y), x);
+    }
+    // the quartet's own block comes last: its gathered rows are v_j here
+    const int base = __ldg(H.base + q);
+    const bool own = last == base;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const size_t e = static_cast<size_t>(base + off[a]) * ldm + t;
+        const double2 vr = cscale(own ? x[a] : src[e], sc);
+        const double2 acc = cscale(o[a], sc);
+        Vj[e] = vr;
+        W[e] = csub(make_double2(acc.y, -acc.x), cscale(vr, kappa));  // -i H v - kappa v
+    }
+}
+
 // Partial dots <V_i, W>, i <= j (the first Gram-Schmidt pass; W unchanged,
 // h unused).  Each V_i is used once and the compiler keeps every load of a
 // row in flight; two CTAs per SM bound its registers.
