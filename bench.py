@@ -597,6 +597,10 @@ def run_dense(args):
                      "unit": "TOP/s" if prec == "int8x4" else "TFLOP/s", "frac": achieved / peak if achieved else None,
                      "traffic": traffic, "peak_kind": peak_note,
                      "flops_per_launch": flops, "avg_launch_ms": gms / gn if gn else None,
+                     # the complex product itself, 8 D^2 flops per trajectory (one complex MAC = 8
+                     # real flops), against the split products the tensor cores execute
+                     "algorithmic_flops_per_launch": 8.0 * D * D * M,
+                     "algorithmic_tflops": (8.0 * D * D * M) / (gms / gn / 1e3) / 1e12 if gn else None,
                      "launches_timed": gn, "timing": "CUDA events around every 8th GEMM (sampled)",
                      "share_of_step": (gms / gn) * chunk * args.steps / el if gn and el else None},
         "accuracy_vs_c128_200_steps": {
