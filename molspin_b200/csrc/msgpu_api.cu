@@ -90,6 +90,10 @@ struct msgpu_ctx {
     // form, built when the quartet form has the nuclear-bit structure
     DevBuf tc_src, tc_tab;
     int tc_P = 0, tc_entries = 0;
+    CUtensorMap tc_map{};      // 2D map over the Krylov basis (boxes of 128 trajectories x TcCfg::HB rows)
+    const void *tc_map_base = nullptr;
+    long long tc_map_rows = 0;
+    int tc_map_ldm = 0;
     long long tc_build = -1;   // quartet build the tables were validated for
     bool tc_ok = false;        // structure present (tables valid)
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
@@ -1549,6 +1553,45 @@ constexpr bool kTcInTuner = false;
 int tc_cube_bits(int v) { return v == kNumSimtVariants ? 4 : 3; }
 
 // U = s H w over `width` trajectories with the tensor-core SpMM.
+using TcEncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The tensor-core SpMM's 2D tensor map over the complex64 Krylov basis:
+// 8-byte elements, rows of ldm trajectories, boxes of 128 trajectories x HB
+// rows; re-encoded when the basis buffer or its shape changes.  On failure the
+// tensor-core variants are switched off for this context (tc_ok = false).
+int tc_prepare_map(msgpu_ctx *c)
+{
+    if (!c->tc_ok || !c->basis.p) return MSGPU_OK;
+    const long long rows = static_cast<long long>(c->basis.bytes / (8 * static_cast<size_t>(c->ldm)));
+    if (c->tc_map_base == c->basis.p && c->tc_map_rows == rows && c->tc_map_ldm == c->ldm) return MSGPU_OK;
+    static TcEncodeTiled enc = nullptr;
+    if (!enc) {
+        void *fp = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            enc = reinterpret_cast<TcEncodeTiled>(fp);
+    }
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(c->ldm), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(c->ldm) * 8};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kTcTraj), static_cast<cuuint32_t>(TcCfg<4>::HB)};
+    const cuuint32_t estr[2] = {1, 1};
+    static_assert(TcCfg<4>::HB == TcCfg<3>::HB, "one box shape");
+    if (!enc || enc(&c->tc_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, c->basis.p, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        c->tc_ok = false;
+        c->tc_map_base = nullptr;
+        return MSGPU_OK;
+    }
+    c->tc_map_base = c->basis.p;
+    c->tc_map_rows = rows;
+    c->tc_map_ldm = c->ldm;
+    return MSGPU_OK;
+}
+
 void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, const double *s, float2 *U, double *part,
                int width)
 {
@@ -1557,16 +1600,19 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
     const unsigned char *tdiag = tflip + static_cast<size_t>(2 * P) * 2 * kTcB;
     const dim3 grid(Q >> cb, ceil_div(width, kTcTraj));
     int *status = static_cast<int *>(c->status.p);
+    // w lies in the basis the map covers (apply_fits checks the map): its first row and column
+    const long long offs = w - static_cast<const float2 *>(c->tc_map_base);
+    const int y0 = static_cast<int>(offs / c->ldm), x0 = static_cast<int>(offs % c->ldm);
     if (cb == 4) {
         const int smem = TcCfg<4>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<4>), smem);
-        k_lanczos_apply_tc<4><<<grid, TcCfg<4>::Threads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
-                                                              width, status);
+        k_lanczos_apply_tc<4><<<grid, TcCfg<4>::Threads, smem, st>>>(c->tc_map, x0, y0, tflip, tdiag, P, c->s1, c->s2, s, U,
+                                                                     part, c->ldm, width, status);
     } else {
         const int smem = TcCfg<3>::smem(P);
         raise_smem_limit(reinterpret_cast<const void *>(k_lanczos_apply_tc<3>), smem);
-        k_lanczos_apply_tc<3><<<grid, TcCfg<3>::Threads, smem, st>>>(tflip, tdiag, P, c->s1, c->s2, w, s, U, part, c->ldm,
-                                                              width, status);
+        k_lanczos_apply_tc<3><<<grid, TcCfg<3>::Threads, smem, st>>>(c->tc_map, x0, y0, tflip, tdiag, P, c->s1, c->s2, s, U,
+                                                                     part, c->ldm, width, status);
     }
 }
 
@@ -1576,7 +1622,10 @@ bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
     *smem = 0;
     if (v >= kNumSimtVariants) {
         const int cb = tc_cube_bits(v);
-        if (!c->tc_ok || qt != (1 << cb) || c->tc_P < cb + 1) return false;
+        // the map covers this basis, and the cube's quartets have consecutive rows (boxes of HB rows)
+        if (!c->tc_ok || qt != (1 << cb) || c->tc_P < cb + 1 || c->s2 % (1 << cb) != 0 || !c->tc_map_base ||
+            c->tc_map_base != c->basis.p || c->tc_map_ldm != c->ldm)
+            return false;
         *smem = static_cast<size_t>(cb == 4 ? TcCfg<4>::smem(c->tc_P) : TcCfg<3>::smem(c->tc_P));
         return true;
     }
@@ -1949,6 +1998,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     if (prec == MSGPU_PREC_C64) {
         if (int rc = build_quartet(c)) return rc;
         if (int rc = build_tc(c)) return rc;
+        if (int rc = tc_prepare_map(c)) return rc;
         fused_c = fused_cluster(c);
         if (!fused_c)
             if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc,

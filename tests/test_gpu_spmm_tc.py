@@ -66,18 +66,26 @@ def test_tc_against_simt_and_complex128(variant):
     assert _rel(val_t, val_d) < 1e-6
 
 
-@pytest.mark.parametrize("variant", TC_VARIANTS)
-def test_tc_interleaved_electrons_small_tile_against_oracle(variant):
-    # electrons at basis positions 1 and 4 of 8 spin-1/2 spins (D = 256, P = 6),
-    # 64 trajectories: one half-filled 128-trajectory tile
+def _interleaved(second: int):
+    # 8 spin-1/2 spins with electrons at basis positions 1 and `second` (D = 256, P = 6)
     rng = np.random.default_rng(12)
-    s = S.SpinSystem(mult=[2] * 8, names=[f"S{i}" for i in range(8)], electrons=(1, 4))
-    for e in (1, 4):
+    s = S.SpinSystem(mult=[2] * 8, names=[f"S{i}" for i in range(8)], electrons=(1, second))
+    for e in (1, second):
         s.linear.append((e, S.COMMON_PREFACTOR * 2.0023 * 1e-4 * rng.normal(size=3)))
-    for e, n in ((1, 0), (1, 2), (1, 3), (4, 5), (4, 6), (1, 7)):
+    nuclei = [n for n in range(8) if n not in (1, second)]
+    for k, n in enumerate(nuclei):
+        e = second if k in (3, 4) else 1
         s.bilinear.append((e, n, S.COMMON_PREFACTOR * 2.0023e-3 * S._aniso_tensor(rng, 2.0)))
     s.sinks = {"S": 2e-3, "T0": 2e-3, "Tp": 2e-3, "Tm": 2e-3}
     assert s.dim == 256
+    return s, rng
+
+
+@pytest.mark.parametrize("variant", TC_VARIANTS)
+def test_tc_interleaved_electrons_small_tile_against_oracle(variant):
+    # electrons at basis positions 1 and 3 (strides 64 and 16: a cube's quartets
+    # still have consecutive rows), 64 trajectories: one half-filled 128-trajectory tile
+    s, rng = _interleaved(3)
     M, times = 64, S.time_grid(40.0, 1.0)
     F = rng.normal(size=(s.dim, M)) + 1j * rng.normal(size=(s.dim, M))
     F /= np.linalg.norm(F, axis=0) * np.sqrt(M)
@@ -146,5 +154,12 @@ def test_tc_refused_without_the_nuclear_bit_structure():
     # variant is refused with an error rather than run
     s = h.random_system([2, 3], [2], seed=3)
     F = s.trace_samples(64, 1.0)
+    with pytest.raises(hs.MsgpuError):
+        _run(s, F, S.time_grid(4.0, 1.0), "c64", 8)
+    # electrons at positions 1 and 4: the second stride is 8, so a 16-quartet
+    # cube's rows are not consecutive and variant 8's boxes cannot load it
+    s, rng = _interleaved(4)
+    F = rng.normal(size=(s.dim, 64)) + 1j * rng.normal(size=(s.dim, 64))
+    F /= np.linalg.norm(F, axis=0) * 8.0
     with pytest.raises(hs.MsgpuError):
         _run(s, F, S.time_grid(4.0, 1.0), "c64", 8)
