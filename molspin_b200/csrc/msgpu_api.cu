@@ -1566,14 +1566,15 @@ int tc_prepare_map(msgpu_ctx *c)
     if (!c->tc_ok || !c->basis.p) return MSGPU_OK;
     const long long rows = static_cast<long long>(c->basis.bytes / (8 * static_cast<size_t>(c->ldm)));
     if (c->tc_map_base == c->basis.p && c->tc_map_rows == rows && c->tc_map_ldm == c->ldm) return MSGPU_OK;
-    static TcEncodeTiled enc = nullptr;
-    if (!enc) {
+    // looked up once (thread-safe static initialisation: batch contexts prepare from several host threads)
+    static const TcEncodeTiled enc = []() -> TcEncodeTiled {
         void *fp = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            enc = reinterpret_cast<TcEncodeTiled>(fp);
-    }
+            return reinterpret_cast<TcEncodeTiled>(fp);
+        return nullptr;
+    }();
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(c->ldm), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(c->ldm) * 8};
     const cuuint32_t box[2] = {static_cast<cuuint32_t>(kTcTraj), static_cast<cuuint32_t>(TcCfg<4>::HB)};

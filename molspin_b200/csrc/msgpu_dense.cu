@@ -939,14 +939,15 @@ using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
 
 EncodeTiled encoder()
 {
-    static EncodeTiled fn = nullptr;
-    if (!fn) {
+    // looked up once; static initialisation is thread-safe (contexts may prepare from several host threads)
+    static const EncodeTiled fn = []() -> EncodeTiled {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiled>(p);
-    }
+            return reinterpret_cast<EncodeTiled>(p);
+        return nullptr;
+    }();
     return fn;
 }
 
