@@ -70,8 +70,8 @@ struct msgpu_ctx {
     // group's SpMM overlaps the other's update and combine on a second stream
     int tgroups_opt = 0;  // 0 auto, else the number of groups asked for
     int combine_tile_opt = 0;  // MSGPU_OPT_COMBINE_TILE: quartets per evaluation tile (0: by dimension)
-    cudaStream_t gside = nullptr;
-    cudaEvent_t gfork = nullptr, gjoin = nullptr;
+    cudaStream_t gside[3] = {nullptr, nullptr, nullptr};  // trajectory groups 1..3 (group 0: the context stream)
+    cudaEvent_t gfork = nullptr, gjoin[3] = {nullptr, nullptr, nullptr};
     // H as a fixed-pattern linear combination of terms (msgpu_upload_hamiltonian_terms):
     // the host copy h_val then holds a generic combination (structure only)
     bool terms = false;
@@ -336,8 +336,10 @@ void msgpu_destroy(msgpu_ctx *c)
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
     if (c->gfork) cudaEventDestroy(c->gfork);
-    if (c->gjoin) cudaEventDestroy(c->gjoin);
-    if (c->gside) cudaStreamDestroy(c->gside);
+    for (int k = 0; k < 3; ++k) {
+        if (c->gjoin[k]) cudaEventDestroy(c->gjoin[k]);
+        if (c->gside[k]) cudaStreamDestroy(c->gside[k]);
+    }
     for (auto &a : c->dense_allocs) cudaFree(a.first);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -2229,18 +2231,23 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             const int G = fused_c ? 1 : traj_groups(c), width = ldm / G;
             const bool timed_step = c->prof == 1 || (c->prof == 2 && c->prof_tick % kProfileEvery == 0);
             const bool overlap = G > 1 && !timed_step;
+            // each group on its own stream (group 0 on the context stream)
+            const int nside = overlap ? G - 1 : 0;
             if (overlap) {
-                if (!c->gside && ((e = cudaStreamCreateWithFlags(&c->gside, cudaStreamNonBlocking)) ||
-                                  (e = cudaEventCreateWithFlags(&c->gfork, cudaEventDisableTiming)) ||
-                                  (e = cudaEventCreateWithFlags(&c->gjoin, cudaEventDisableTiming))))
+                if (!c->gfork && (e = cudaEventCreateWithFlags(&c->gfork, cudaEventDisableTiming)))
                     return cuda_fail(c, e, "trajectory group stream");
-                if ((e = cudaEventRecord(c->gfork, st)) || (e = cudaStreamWaitEvent(c->gside, c->gfork, 0)))
-                    return cuda_fail(c, e, "trajectory group fork");
+                for (int k = 0; k < nside; ++k)
+                    if (!c->gside[k] && ((e = cudaStreamCreateWithFlags(&c->gside[k], cudaStreamNonBlocking)) ||
+                                         (e = cudaEventCreateWithFlags(&c->gjoin[k], cudaEventDisableTiming))))
+                        return cuda_fail(c, e, "trajectory group stream");
+                if ((e = cudaEventRecord(c->gfork, st))) return cuda_fail(c, e, "trajectory group fork");
+                for (int k = 0; k < nside; ++k)
+                    if ((e = cudaStreamWaitEvent(c->gside[k], c->gfork, 0))) return cuda_fail(c, e, "trajectory group fork");
             }
             for (int gi = 0; gi < G; ++gi) {
                 const int t0 = gi * width;
                 const size_t tm0 = static_cast<size_t>(t0) * mws;  // offset into the [t][m] T arrays
-                cudaStream_t gs = (overlap && (gi & 1)) ? c->gside : st;
+                cudaStream_t gs = (overlap && gi > 0) ? c->gside[gi - 1] : st;
                 dim3 grid(nt, width / 64);
                 for (int j = 0; j < (fused_c ? 0 : m); ++j) {
                     {
@@ -2283,8 +2290,9 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                         s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, qobs + t0, qnrm + t0);
                 }
             }
-            if (overlap && ((e = cudaEventRecord(c->gjoin, c->gside)) || (e = cudaStreamWaitEvent(st, c->gjoin, 0))))
-                return cuda_fail(c, e, "trajectory group join");
+            for (int k = 0; k < nside; ++k)
+                if ((e = cudaEventRecord(c->gjoin[k], c->gside[k])) || (e = cudaStreamWaitEvent(st, c->gjoin[k], 0)))
+                    return cuda_fail(c, e, "trajectory group join");
         }
         yield_update(dt, 0, s + 1);
         if ((e = cudaGetLastError())) return cuda_fail(c, e, "step launch");
