@@ -90,8 +90,10 @@ extern "C" {
                                         that stage the tile's own quartets in shared memory,
                                         6-7 two trajectory pairs per thread, 8-9 the
                                         tensor-core SpMM over cubes of 16 / 8 quartets, for
-                                        radical pairs whose other spins are all spin-1/2;
-                                        refused with MSGPU_ERR_INVALID at the run otherwise);
+                                        radical pairs whose other spins are all spin-1/2 and
+                                        whose second electron stride is a multiple of the
+                                        cube; refused with MSGPU_ERR_INVALID at the run
+                                        otherwise);
                                         a forced variant also keeps the four-kernel Lanczos
                                         iteration */
 #define MSGPU_OPT_TAYLOR_TOL 2        /* truncation tolerance of MSGPU_PROP_TAYLOR: 2^-53
