@@ -46,8 +46,11 @@ extern "C" {
 #define MSGPU_PREC_C64 1  /* precision form: complex64 vectors and H, FP64 reductions, expm and sums */
 
 /* Krylov recurrences. */
-#define MSGPU_REC_AUTO 0    /* Arnoldi for C128, Lanczos for C64 with scalar K */
-#define MSGPU_REC_ARNOLDI 1 /* Arnoldi on G = -iH - K (as SpinSpace::ArnoldiProcess) */
+#define MSGPU_REC_AUTO 0    /* Arnoldi for C128; for C64 Lanczos with scalar K, else Arnoldi */
+#define MSGPU_REC_ARNOLDI 1 /* Arnoldi on G = -iH - K (as SpinSpace::ArnoldiProcess).  C64
+                               takes it when K acts on the electron pair only (K = I x K4,
+                               e.g. unequal sinks on the pair's states: CGS2 with FP64 dots,
+                               FP32 storage); any other K needs C128 */
 #define MSGPU_REC_LANCZOS 2 /* Lanczos on H; valid only when K is a scalar */
 
 /* Propagators. */

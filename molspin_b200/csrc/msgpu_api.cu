@@ -107,6 +107,10 @@ struct msgpu_ctx {
     int dense_renorm = 1;
     // reaction
     bool k_scalar = true;
+    // host copy of a CSR K (interleaved complex values): the complex64 Arnoldi form
+    // checks on it that K acts on the electron pair only
+    std::vector<int> k_hrow, k_hcol;
+    std::vector<double> k_hval;
     double kappa = 0.0;
     double2 k_trace = {0.0, 0.0};  // trace of a CSR K
     double k_norm1 = 0.0;          // its 1-norm (max column sum)
@@ -512,6 +516,9 @@ int msgpu_upload_reaction_csr(msgpu_ctx *c, const int *rowptr, const int *col, c
         (e = cudaStreamSynchronize(c->stream)))
         return cuda_fail(c, e, "reaction upload");
     c->k_scalar = false;
+    c->k_hrow.assign(rowptr, rowptr + D + 1);
+    c->k_hcol.assign(col, col + nnz);
+    c->k_hval.assign(val, val + 2 * static_cast<size_t>(nnz));
     // trace and 1-norm (max column sum) for the Taylor propagator's shift and sub-steps
     std::vector<double> colsum(D, 0.0);
     c->k_trace = make_double2(0.0, 0.0);
@@ -906,6 +913,44 @@ int resident_warps(const msgpu_ctx *c, int prec, int m)
     const int spread = std::max(1, c->M / sms);
     const int w = static_cast<int>(std::min<size_t>(std::min(4, spread), kResidentSmemBudget / wb));
     return w;
+}
+
+// K as I (x) K4 on the electron pair (the 4 x 4 block in the pair index
+// a = 2 a1 + a2, a1 the digit of stride s1): true when every quartet's rows
+// couple only to the same quartet, with the same block (to 1e-12 of the
+// largest entry).  A scalar K is kappa I.
+bool pair_reaction(const msgpu_ctx *c, PairK *out)
+{
+    for (int i = 0; i < 16; ++i) out->k[i] = make_double2(0.0, 0.0);
+    if (c->k_scalar) {
+        for (int a = 0; a < 4; ++a) out->k[5 * a] = make_double2(c->kappa, 0.0);
+        return true;
+    }
+    const int D = c->D, s1 = c->s1, s2 = c->s2;
+    if (static_cast<int>(c->k_hrow.size()) != D + 1 || s1 <= 0 || s2 <= 0) return false;
+    double kmax = 0.0;
+    for (size_t k = 0; k < c->k_hcol.size(); ++k) kmax = std::max(kmax, std::hypot(c->k_hval[2 * k], c->k_hval[2 * k + 1]));
+    const double tol = 1e-12 * kmax;
+    bool have[4] = {false, false, false, false};
+    for (int r = 0; r < D; ++r) {
+        const int a1 = (r / s1) & 1, a2 = (r / s2) & 1, a = 2 * a1 + a2;
+        const int base = r - a1 * s1 - a2 * s2;
+        double row[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+        for (int k = c->k_hrow[r]; k < c->k_hrow[r + 1]; ++k) {
+            const int col = c->k_hcol[k];
+            const int b1 = (col / s1) & 1, b2 = (col / s2) & 1;
+            if (col - b1 * s1 - b2 * s2 != base) return false;  // leaves the quartet
+            row[2 * b1 + b2][0] += c->k_hval[2 * static_cast<size_t>(k)];
+            row[2 * b1 + b2][1] += c->k_hval[2 * static_cast<size_t>(k) + 1];
+        }
+        for (int b = 0; b < 4; ++b) {
+            double2 &kk = out->k[4 * a + b];
+            if (!have[a]) kk = make_double2(row[b][0], row[b][1]);
+            else if (std::abs(kk.x - row[b][0]) > tol || std::abs(kk.y - row[b][1]) > tol) return false;
+        }
+        have[a] = true;
+    }
+    return true;
 }
 
 int run_resident(msgpu_ctx *c, const msgpu_run_params *p, int prec, int m)
@@ -1905,8 +1950,11 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         rec = (p->precision == MSGPU_PREC_C64 && c->k_scalar) ? MSGPU_REC_LANCZOS : MSGPU_REC_ARNOLDI;
     if (rec == MSGPU_REC_LANCZOS && !c->k_scalar)
         return fail(c, MSGPU_ERR_INVALID, "run: Lanczos requires a scalar reaction operator K");
-    if (p->precision == MSGPU_PREC_C64 && rec != MSGPU_REC_LANCZOS)
-        return fail(c, MSGPU_ERR_INVALID, "run: the complex64 form implements the Lanczos recurrence only");
+    PairK pair_k{};  // K on the electron pair, for the complex64 Arnoldi form
+    if (p->precision == MSGPU_PREC_C64 && rec == MSGPU_REC_ARNOLDI && !pair_reaction(c, &pair_k))
+        return fail(c, MSGPU_ERR_INVALID,
+                    "run: the complex64 Arnoldi form needs K acting on the electron pair only (K = I x K4, e.g. "
+                    "unequal sinks on the pair's states); use complex128 for a general K");
     if (p->precision == MSGPU_PREC_C128 && rec != MSGPU_REC_ARNOLDI)
         return fail(c, MSGPU_ERR_INVALID, "run: the complex128 form implements the Arnoldi recurrence only");
     if (c->noise_mode == MSGPU_NOISE_REPLAY) {
@@ -1933,6 +1981,14 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
             if (int rc = ensure_state(c, MSGPU_PREC_C128)) return rc;
     }
     if (int rc = ensure_workspace(c, prec, m)) return rc;
+    if (prec == MSGPU_PREC_C64 && rec == MSGPU_REC_ARNOLDI) {
+        // the complex64 Arnoldi form's Hessenberg matrices, dots and Gram-Schmidt partials
+        int rc;
+        if ((rc = ensure(c, c->hess, static_cast<size_t>(ldm) * m * m * sizeof(double2), "Hessenberg")) ||
+            (rc = ensure(c, c->part2, static_cast<size_t>(3) * (m + 1) * ldm * sizeof(double2), "dots")) ||
+            (rc = ensure(c, c->wbuf, static_cast<size_t>(c->ntiles) * (m + 1) * ldm * sizeof(double2), "partials")))
+            return rc;
+    }
     if (int rc = ensure_state(c, prec)) return rc;
     const int mws = m;  // layout stride of the per-trajectory Krylov arrays
     cudaError_t e;
@@ -1994,6 +2050,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     }
     yield_update(0.0, 1, 0);
     int fused_c = 0;  // cluster size of k_lanczos_fused, 0: the four-kernel iteration
+    const bool arn64 = prec == MSGPU_PREC_C64 && rec == MSGPU_REC_ARNOLDI;
     // the complex128 Arnoldi apply runs over quartet blocks when K = kappa I
     const bool quartet128 = prec == MSGPU_PREC_C128 && !taylor && !rk4 && c->k_scalar;
     if (quartet128)
@@ -2002,7 +2059,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
         if (int rc = build_quartet(c)) return rc;
         if (int rc = build_tc(c)) return rc;
         if (int rc = tc_prepare_map(c)) return rc;
-        fused_c = fused_cluster(c);
+        fused_c = arn64 ? 0 : fused_cluster(c);
         if (!fused_c)
             if (int rc = tune_quartet_tile(c, static_cast<const float2 *>(c->basis.p), sc,
                                            static_cast<float2 *>(c->ubuf.p), static_cast<double *>(c->part.p)))
@@ -2208,6 +2265,51 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                     static_cast<int *>(c->mdim.p), mws, c->s1, c->s2, Q, ldm, QR, nz, g, 1, pstep(s),
                     s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po, static_cast<double *>(c->qpart_obs.p),
                     static_cast<double *>(c->qpart_nrm.p));
+            }
+        } else if (arn64) {
+            // complex64 Arnoldi (CGS2) for K = I (x) K4: basis slot j holds w_j with
+            // scale sc[j] = 1/|w_j|, as the Lanczos form; one trajectory group
+            float2 *Wb = static_cast<float2 *>(c->basis.p);
+            float2 *U = static_cast<float2 *>(c->ubuf.p);
+            double2 *dots = static_cast<double2 *>(c->part2.p);  // [3][m+1][ldm]: h1, h2, norm
+            double2 *h1 = dots, *h2 = dots + static_cast<size_t>(m + 1) * ldm, *nr = dots + 2 * static_cast<size_t>(m + 1) * ldm;
+            double2 *apart = static_cast<double2 *>(c->wbuf.p);  // Gram-Schmidt partials [tile][i][t]
+            const int QT = c->q_tile;
+            const dim3 ogrid(nt, ldm / 32);
+            for (int j = 0; j < m; ++j) {
+                float2 *Wn = Wb + static_cast<size_t>(j + 1) * n;
+                {
+                    Timed tm(c, KC_APPLY);
+                    launch_apply(c, c->q_variant, QT, dim3(ceil_div(Q, std::max(1, QT))), st, Wb + j * n,
+                                 sc + static_cast<size_t>(j) * ldm, U, static_cast<double *>(c->part.p), ldm);
+                    k_arn64_apply<<<dim3(ceil_div(Q, kWarps), ldm / 64), kThreads, 0, st>>>(
+                        pair_k, U, Wb + j * n, sc + static_cast<size_t>(j) * ldm, Wn, Q, c->s1, c->s2, ldm);
+                }
+                {
+                    Timed tm(c, KC_ORTH);
+                    arn64_orth_fn(j, 0)<<<ogrid, kThreads, 0, st>>>(Wn, Wb, n, sc, nullptr, apart, D, ldm, R);
+                    k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(apart, nt, j + 1, ldm, h1);
+                    arn64_orth_fn(j, 1)<<<ogrid, kThreads, 0, st>>>(Wn, Wb, n, sc, h1, apart, D, ldm, R);
+                    k_reduce_partials<<<dim3(ldm / 32, j + 1), dim3(32, 8), 0, st>>>(apart, nt, j + 1, ldm, h2);
+                    arn64_orth_fn(j, 2)<<<ogrid, kThreads, 0, st>>>(Wn, Wb, n, sc, h2, apart, D, ldm, R);
+                    k_reduce_partials<<<dim3(ldm / 32, 1), dim3(32, 8), 0, st>>>(apart, nt, 1, ldm, nr);
+                    k_arnoldi_finalize<<<ceil_div(ldm, 256), 256, 0, st>>>(
+                        h1, h2, nr, j, mws, ldm, static_cast<double2 *>(c->hess.p), static_cast<int *>(c->mdim.p),
+                        sc + static_cast<size_t>(j + 1) * ldm);
+                }
+            }
+            {
+                Timed tm(c, KC_EXPM);
+                k_krylov_expm<<<ceil_div(ldm, expm_warps), 32 * expm_warps, expm_warps * expm_smem_warp, st>>>(
+                    static_cast<double2 *>(c->hess.p), nullptr, nullptr, 0.0, static_cast<int *>(c->mdim.p), beta0, sc,
+                    mws, ldm, M, dt, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->status.p));
+            }
+            {
+                Timed tm(c, KC_COMBINE);
+                k_combine_pp<true><<<dim3(qt, ldm / 64), qblock, 0, st>>>(
+                    Wb, Wb, n, static_cast<double2 *>(c->coef.p), static_cast<int *>(c->mdim.p), c->s1, c->s2, Q, ldm,
+                    QR, nz, g, 1, pstep(s), s + 1 < steps ? g + 1 : -1, 0, pstep(s + 1), po,
+                    static_cast<double *>(c->qpart_obs.p), static_cast<double *>(c->qpart_nrm.p));
             }
         } else {
             float2 *Wb = static_cast<float2 *>(c->basis.p);  // w_0 = state

@@ -295,6 +295,138 @@ k_arnoldi_orth(double2 *__restrict__ W, const double2 *__restrict__ V, size_t vs
     }
 }
 
+// ------------------------------------------------ complex64 Arnoldi (general K on the pair)
+// The complex64 form for a reaction operator K = I (x) K4 that acts on the
+// electron pair only (unequal sinks: K = sum_c k_c/2 P_c).  Basis slot j holds
+// w_j unnormalised in the pair-planar layout, with the per-trajectory scale
+// s_j = 1 / |w_j| (v_j = s_j w_j), as in the Lanczos form; the quartet SpMM
+// gives U = H v_j.  Arithmetic in FP64 (FP32 storage), one trajectory per lane:
+// a lane reads its trajectory's re and im words of the pair's 16 bytes.
+
+struct PairK {
+    double2 k[16];  // K4, row-major in the pair index a = 2 a1 + a2
+};
+
+// W = -i U - K4 v_j per quartet, stored as w_{j+1} (before orthogonalisation).
+// Grid (ceil(Q / 8), ldm / 64), 256 threads: a warp per quartet, a lane per
+// trajectory pair.
+__global__ void __launch_bounds__(kThreads)
+k_arn64_apply(PairK K, const float2 *__restrict__ U, const float2 *__restrict__ wj, const double *__restrict__ sj,
+              float2 *__restrict__ W, int Q, int s1, int s2, int ldm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 64 + 2 * lane;
+    const int q = blockIdx.x * kWarps + warp;
+    if (q >= Q) return;
+    const int base = quartet_base(q, s1, s2);
+    const int off[4] = {0, s2, s1, s1 + s2};
+    const double sc0 = sj[t], sc1 = sj[t + 1];
+    double2 v[2][4], u[2][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const size_t e = static_cast<size_t>(base + off[a]) * ldm + t;
+        const float4 x = *reinterpret_cast<const float4 *>(wj + e);
+        const float4 h = *reinterpret_cast<const float4 *>(U + e);
+        v[0][a] = make_double2(x.x * sc0, x.z * sc0);
+        v[1][a] = make_double2(x.y * sc1, x.w * sc1);
+        u[0][a] = make_double2(h.x, h.z);
+        u[1][a] = make_double2(h.y, h.w);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        double2 g[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            double2 kv = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) kv = cfma(K.k[4 * a + b], v[k][b], kv);
+            g[k] = csub(make_double2(u[k][a].y, -u[k][a].x), kv);  // -i U - K v
+        }
+        *reinterpret_cast<float4 *>(W + static_cast<size_t>(base + off[a]) * ldm + t) =
+            make_float4(static_cast<float>(g[0].x), static_cast<float>(g[1].x), static_cast<float>(g[0].y),
+                        static_cast<float>(g[1].y));
+    }
+}
+
+// MODE 0: partial dots <v_i, W>, i <= J; MODE 1: W -= sum_i h_i v_i, then the
+// dots again; MODE 2: W -= sum_i h_i v_i, then |W|^2 (in .x).  v_i = s_i w_i
+// from the basis slots: the update uses h_i s_i and the dots scale by s_i once
+// at the end, so the per-element work is that of the complex128 kernels.
+// Grid (ntiles, ldm / 32), a lane per trajectory (its re and im words of the
+// pair's 16 bytes).  Partials go to part[tile][i][t] (the layout of the
+// complex128 kernels).
+template <int J, int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_arn64_orth(float2 *__restrict__ W, const float2 *__restrict__ V, size_t vstride, const double *__restrict__ sc,
+             const double2 *__restrict__ h, double2 *__restrict__ part, int D, int ldm, int R)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int t = blockIdx.y * 32 + lane;
+    const int r0 = blockIdx.x * R;
+    // per-trajectory h_i s_i and s_i, once per CTA
+    __shared__ double2 hs[J + 1][32];
+    __shared__ double si[J + 1][32];
+    for (int k = threadIdx.x; k < (J + 1) * 32; k += kThreads) {
+        const size_t e = static_cast<size_t>(k >> 5) * ldm + blockIdx.y * 32 + (k & 31);
+        si[k >> 5][k & 31] = sc[e];
+        hs[k >> 5][k & 31] = MODE == 0 ? make_double2(0.0, 0.0) : cscale(h[e], sc[e]);
+    }
+    __syncthreads();
+    constexpr int ND = MODE == 2 ? 1 : J + 1;
+    double2 dacc[ND];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) dacc[i] = make_double2(0.0, 0.0);
+    auto ld = [&](const float2 *x, int r) {
+        const float *f = reinterpret_cast<const float *>(x + static_cast<size_t>(r) * ldm + (t & ~1)) + (t & 1);
+        return make_double2(f[0], f[2]);
+    };
+    for (int r = r0 + warp; r < min(r0 + R, D); r += kWarps) {
+        double2 w = ld(W, r);
+        if (MODE != 0) {
+#pragma unroll
+            for (int i = 0; i <= J; ++i) w = csub(w, cmul(hs[i][lane], ld(V + i * vstride, r)));
+            float *f = reinterpret_cast<float *>(W + static_cast<size_t>(r) * ldm + (t & ~1)) + (t & 1);
+            f[0] = static_cast<float>(w.x);
+            f[2] = static_cast<float>(w.y);
+            w = make_double2(f[0], f[2]);  // the stored (rounded) vector is the one the next pass sees
+        }
+        if (MODE != 2) {
+#pragma unroll
+            for (int i = 0; i <= J; ++i) dacc[i] = cadd(dacc[i], cconjmul(ld(V + i * vstride, r), w));
+        } else {
+            dacc[0].x += cabs2(w);
+        }
+    }
+    __shared__ double2 sm[kWarps][32];
+#pragma unroll  // static indices keep dacc in registers
+    for (int i = 0; i < ND; ++i) {
+        sm[warp][lane] = MODE == 2 ? dacc[i] : cscale(dacc[i], si[i][lane]);
+        __syncthreads();
+        if (warp == 0) {
+            double2 s = sm[0][lane];
+            for (int w2 = 1; w2 < kWarps; ++w2) s = cadd(s, sm[w2][lane]);
+            part[(static_cast<size_t>(blockIdx.x) * ND + i) * ldm + t] = s;
+        }
+        __syncthreads();
+    }
+}
+
+using Arn64Fn = void (*)(float2 *, const float2 *, size_t, const double *, const double2 *, double2 *, int, int, int);
+template <int J, int MODE>
+constexpr Arn64Fn arn64_kernel() { return &k_arn64_orth<J, MODE>; }
+template <int MODE, int... J>
+Arn64Fn arn64_pick(int j, std::integer_sequence<int, J...>)
+{
+    static constexpr Arn64Fn table[] = {arn64_kernel<J, MODE>()...};
+    return table[j];
+}
+// The complex64 Gram-Schmidt kernel of iteration j (0 <= j < kMaxKrylov), mode 0, 1 or 2.
+inline Arn64Fn arn64_orth_fn(int j, int mode)
+{
+    constexpr auto js = std::make_integer_sequence<int, kMaxKrylov>{};
+    return mode == 0 ? arn64_pick<0>(j, js) : mode == 1 ? arn64_pick<1>(j, js) : arn64_pick<2>(j, js);
+}
+
 using ArnoldiOrthFn = void (*)(double2 *, const double2 *, size_t, const double2 *, double2 *, int, int, int);
 
 template <int J, int MODE>

@@ -309,3 +309,63 @@ def test_shared_memory_spmm_variants(variant):
     reg = run("c64", 3)
     assert _rel(cube, ref128) < 1e-6
     assert _rel(cube, reg) < 1e-6
+
+
+def _unequal_sinks_system(n_a, n_b, seed):
+    s = h.random_system(n_a, n_b, seed=seed, aniso=True, st_rate=0.05)
+    s.sinks = {"S": 3e-3, "T0": 1e-3, "Tp": 0.5e-3, "Tm": 2e-3}
+    K = sum(0.5 * rate * den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), s) for n, rate in s.sinks.items())
+    return s, den.to_csr(K, 1e-18)
+
+
+def test_complex64_arnoldi_unequal_sinks_against_oracle():
+    # unequal sinks make K = sum_c k_c/2 P_c a non-scalar operator on the pair:
+    # the complex64 form runs Arnoldi (CGS2, FP64 dots, FP32 storage) and
+    # matches the oracle's complex128 MGS Arnoldi within 1e-6 (a spin-1
+    # nucleus, interleaved electrons)
+    s = S.SpinSystem(mult=[2, 2, 3, 2, 2], names=["N1", "E1", "N2", "E2", "N3"], electrons=(1, 3))
+    rng = np.random.default_rng(4)
+    for e in (1, 3):
+        s.linear.append((e, S.COMMON_PREFACTOR * 2.0023 * 1e-4 * rng.normal(size=3)))
+    for e, n in ((1, 0), (1, 2), (3, 4)):
+        s.bilinear.append((e, n, S.COMMON_PREFACTOR * 2.0023e-3 * S._aniso_tensor(rng, 2.0)))
+    s.sinks = {"S": 3e-3, "T0": 1e-3, "Tp": 1e-3, "Tm": 1e-3}
+    s.st_rate = 0.0
+    K = sum(0.5 * rate * den.pair_operator(S.pair_projector(S.PAIR_STATES[n]), s) for n, rate in s.sinks.items())
+    Kc = den.to_csr(K, 1e-18)
+    M = 45
+    F = rng.normal(size=(s.dim, M)) + 1j * rng.normal(size=(s.dim, M))
+    F /= np.linalg.norm(F, axis=0) * math.sqrt(M)
+    times = S.time_grid(30.0, 1.0)
+    obs = [(op, rate) for _, op, rate in s.observables()]
+    per, ens, vals, _ = _gpu(s, F, times, 10, precision="c64", K_csr=Kc, obs=obs, form="streamed")
+    ref = orc.hs_stochastic(s.hamiltonian_csr(), F, times, h.oracle_observables(s), K_csr=Kc, krylov=10)
+    assert _rel(per, ref["traj_yield"]) < 1e-6
+    assert _rel(vals, ref["values"]) < 1e-6
+
+
+def test_complex64_arnoldi_against_complex128_at_d1024():
+    # D = 1024, unequal sinks, Philox ST noise, 256 trajectories over 60 steps:
+    # complex64 Arnoldi against complex128 Arnoldi within the precision form's 1e-6
+    s, Kc = _unequal_sinks_system([2] * 5, [2] * 3, 33)
+    M, times = 256, S.time_grid(60.0, 1.0)
+    F = s.trace_samples(M, 3.0)
+    noise = (s.st_rate, L.NOISE_PHILOX, 19)
+    per64, ens64, val64, _ = _gpu(s, F, times, 16, precision="c64", K_csr=Kc, noise=noise, form="streamed")
+    per128, ens128, val128, _ = _gpu(s, F, times, 16, precision="c128", K_csr=Kc, noise=noise, form="streamed")
+    assert _rel(per64, per128) < 1e-6
+    assert np.max(np.abs(ens64 - ens128) / np.abs(ens128)) < 1e-6
+    assert _rel(val64, val128) < 1e-6
+
+
+def test_complex64_refuses_a_K_beyond_the_pair():
+    # a K that couples nuclear states is not I x K4: complex64 refuses it, complex128 runs it
+    s, Kc = _unequal_sinks_system([2, 2], [2], 35)
+    r, c, v = Kc
+    v = np.array(v, copy=True)
+    v[0] *= 1.5  # the first quartet's block differs from the others
+    F = s.trace_samples(64, 1.0)
+    with pytest.raises(hs.MsgpuError) as e:
+        _gpu(s, F, S.time_grid(3.0, 1.0), 8, precision="c64", K_csr=(r, c, v), form="streamed")
+    assert e.value.code == L.MSGPU_ERR_INVALID
+    _gpu(s, F, S.time_grid(3.0, 1.0), 8, precision="c128", K_csr=(r, c, v), form="streamed")
