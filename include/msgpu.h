@@ -92,10 +92,13 @@ extern "C" {
                                         only (0-3 register-gather variants, 4-5 the variants
                                         that stage the tile's own quartets in shared memory,
                                         6-7 two trajectory pairs per thread, 8-9 the
-                                        tensor-core SpMM over cubes of 16 / 8 quartets, for
-                                        radical pairs whose other spins are all spin-1/2 and
-                                        whose second electron stride is a multiple of the
-                                        cube; refused with MSGPU_ERR_INVALID at the run
+                                        tensor-core SpMM over cubes of 16 / 8 quartets, 10
+                                        the TMEM-staged SpMM (persistent, cubes of 8
+                                        quartets x 256 trajectories, inputs through TMA,
+                                        tcgen05.cp and tcgen05.ld); 8-10 need radical pairs
+                                        whose other spins are all spin-1/2 and whose second
+                                        electron stride is a multiple of the cube, and are
+                                        refused with MSGPU_ERR_INVALID at the run
                                         otherwise);
                                         a forced variant also keeps the four-kernel Lanczos
                                         iteration */

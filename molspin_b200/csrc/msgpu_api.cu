@@ -18,6 +18,7 @@
 #include "msgpu_kernels.cuh"
 #include "msgpu_resident.cuh"
 #include "msgpu_spmm_tc.cuh"
+#include "msgpu_spmm_tm.cuh"
 
 using namespace msgpu;
 
@@ -28,7 +29,8 @@ enum KClass {
     KC_N = 8
 };
 constexpr int kNumSimtVariants = 8;  // entries of kApplyVariants (checked there)
-constexpr int kNumSpmmVariants = kNumSimtVariants + 2;  // + the tensor-core SpMM, cube bits 4 and 3
+constexpr int kNumSpmmVariants = kNumSimtVariants + 3;  // + the tensor-core SpMM (cube bits 4, 3), the TMEM-staged one
+constexpr int kTmVariant = kNumSimtVariants + 2;
 
 struct DevBuf {
     void *p = nullptr;
@@ -89,11 +91,15 @@ struct msgpu_ctx {
     // tensor-core SpMM (k_lanczos_apply_tc): B-operand tables of the quartet
     // form, built when the quartet form has the nuclear-bit structure
     DevBuf tc_src, tc_tab;
+    DevBuf tm_tab;             // block table of the TMEM-staged SpMM (k_tm_tables)
     int tc_P = 0, tc_entries = 0;
     CUtensorMap tc_map{};      // 2D map over the Krylov basis (boxes of 128 trajectories x TcCfg::HB rows)
     const void *tc_map_base = nullptr;
     long long tc_map_rows = 0;
     int tc_map_ldm = 0;
+    CUtensorMap tm_map{};      // the same basis in boxes of 256 trajectories x 8 rows (k_lanczos_apply_tm)
+    bool tm_map_ok = false;
+    int sm_count = 0;          // SMs of the device (persistent SpMM grid)
     long long tc_build = -1;   // quartet build the tables were validated for
     bool tc_ok = false;        // structure present (tables valid)
     int q_tile = 0, q_tile_ldm = 0;  // autotuned quartets per CTA (and the ldm it was tuned for)
@@ -315,6 +321,7 @@ msgpu_ctx *msgpu_create(int device, size_t hbm_budget_bytes)
         delete c;
         return nullptr;
     }
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) c->sm_count = 0;
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return nullptr;
@@ -335,7 +342,7 @@ void msgpu_destroy(msgpu_ctx *c)
                      &c->tdiag, &c->toff, &c->coef, &c->mdim, &c->scale, &c->alpha, &c->beta0, &c->qpart_obs,
                      &c->qpart_nrm, &c->prev, &c->acc, &c->comp, &c->rates_d, &c->status, &c->values_d,
                      &c->colbuf, &c->trajval, &c->times_d, &c->pflip_d, &c->sys_d, &c->work_d, &c->obs_d,
-                     &c->dense_part, &c->hterms, &c->qsrc, &c->tc_src, &c->tc_tab};
+                     &c->dense_part, &c->hterms, &c->qsrc, &c->tc_src, &c->tc_tab, &c->tm_tab};
     for (DevBuf *b : all) release(c, *b);
     msgpu::dense_release(c->dense, dense_release_cb, c);  // its stream and events, then its buffers
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -1095,6 +1102,9 @@ int tc_tables(msgpu_ctx *c)
     k_tc_tables<<<c->tc_entries, 128, 0, c->stream>>>(static_cast<const int2 *>(c->tc_src.p), c->tc_entries,
                                                       static_cast<const float4 *>(c->qval.p),
                                                       static_cast<unsigned char *>(c->tc_tab.p));
+    k_tm_tables<<<ceil_div(8 * c->tc_entries, 256), 256, 0, c->stream>>>(
+        static_cast<const int2 *>(c->tc_src.p), 2 * c->tc_P, c->tc_entries, static_cast<const float4 *>(c->qval.p),
+        static_cast<float4 *>(c->tm_tab.p));
     const cudaError_t e = cudaGetLastError();
     return e ? cuda_fail(c, e, "tensor-core SpMM tables") : MSGPU_OK;
 }
@@ -1348,7 +1358,8 @@ int build_tc(msgpu_ctx *c)
         if (mask[q] != mask[0]) return MSGPU_OK;
     int rc;
     if ((rc = ensure(c, c->tc_src, sizeof(int2) * nent, "tensor-core SpMM table entries")) ||
-        (rc = ensure(c, c->tc_tab, static_cast<size_t>(nent) * 2 * kTcB, "tensor-core SpMM tables")))
+        (rc = ensure(c, c->tc_tab, static_cast<size_t>(nent) * 2 * kTcB, "tensor-core SpMM tables")) ||
+        (rc = ensure(c, c->tm_tab, static_cast<size_t>(nent) * 8 * sizeof(float4), "TMEM-staged SpMM tables")))
         return rc;
     cudaError_t e;
     if ((e = cudaMemcpyAsync(c->tc_src.p, src.data(), sizeof(int2) * nent, cudaMemcpyHostToDevice, c->stream)) ||
@@ -1596,8 +1607,14 @@ constexpr int kCubeMaxQT = 64;  // 128 KB of shared memory
 // 4 / 3) takes part in the tuner's choice; it can always be forced with
 // MSGPU_OPT_SPMM_VARIANT.
 constexpr bool kTcInTuner = false;
+// The TMEM-staged SpMM (variant kTmVariant): cubes of 8 quartets, two compute
+// warpgroups, three copy warps.
+using TmK = TmCfg<3, 2, 3>;
+constexpr bool kTmInTuner = false;
 
 int tc_cube_bits(int v) { return v == kNumSimtVariants ? 4 : 3; }
+
+bool in_tuner(int v) { return v < kNumSimtVariants || (v == kTmVariant ? kTmInTuner : kTcInTuner); }
 
 // U = s H w over `width` trajectories with the tensor-core SpMM.
 using TcEncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -1634,6 +1651,11 @@ int tc_prepare_map(msgpu_ctx *c)
         c->tc_map_base = nullptr;
         return MSGPU_OK;
     }
+    // the TMEM-staged SpMM's boxes: 256 trajectories x one cube of 8 quartet rows
+    const cuuint32_t tbox[2] = {static_cast<cuuint32_t>(TmK::Traj), static_cast<cuuint32_t>(TmK::NQ)};
+    c->tm_map_ok = enc(&c->tm_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, c->basis.p, dims, strides, tbox, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     c->tc_map_base = c->basis.p;
     c->tc_map_rows = rows;
     c->tc_map_ldm = c->ldm;
@@ -1664,10 +1686,37 @@ void launch_tc(const msgpu_ctx *c, int cb, cudaStream_t st, const float2 *w, con
     }
 }
 
+// U = s H w over `width` trajectories with the TMEM-staged SpMM: one
+// persistent CTA per SM (at most one per item).
+void launch_tm(const msgpu_ctx *c, cudaStream_t st, const float2 *w, const double *s, float2 *U, double *part,
+               int width)
+{
+    const int Q = c->D / 4, P = c->tc_P;
+    const int items = (Q / TmK::NQ) * ceil_div(width, TmK::Traj);
+    const int grid = std::max(1, std::min(items, c->sm_count));
+    const long long offs = w - static_cast<const float2 *>(c->tc_map_base);
+    const int y0 = static_cast<int>(offs / c->ldm), x0 = static_cast<int>(offs % c->ldm);
+    auto fn = k_lanczos_apply_tm<3, 2, 3>;
+    raise_smem_limit(reinterpret_cast<const void *>(fn), TmK::Smem);
+    fn<<<grid, TmK::Threads, TmK::Smem, st>>>(c->tm_map, x0, y0, static_cast<const int2 *>(c->tc_src.p),
+                                              static_cast<const float4 *>(c->tm_tab.p), P, c->s1, c->s2, s, U, part,
+                                              c->ldm, width, static_cast<int *>(c->status.p));
+}
+
 // Whether variant v can run with tile QT on this system, and its shared memory.
 bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 {
     *smem = 0;
+    if (v == kTmVariant) {
+        // the maps cover this basis, a cube's 8 quartets have consecutive rows, and a
+        // group's width is a multiple of 64 trajectories
+        if (!c->tc_ok || !c->tm_map_ok || qt != TmK::NQ || c->tc_P < 4 || c->s2 % TmK::NQ != 0 ||
+            !c->tc_map_base || c->tc_map_base != c->basis.p || c->tc_map_ldm != c->ldm || c->sm_count < 1 ||
+            (c->ldm / traj_groups(c)) % 64 != 0)
+            return false;
+        *smem = static_cast<size_t>(TmK::Smem);
+        return true;
+    }
     if (v >= kNumSimtVariants) {
         const int cb = tc_cube_bits(v);
         // the map covers this basis, and the cube's quartets have consecutive rows (boxes of HB rows)
@@ -1691,6 +1740,10 @@ bool apply_fits(const msgpu_ctx *c, int v, int qt, size_t *smem)
 void launch_apply(const msgpu_ctx *c, int v, int qt, dim3 grid, cudaStream_t st, const float2 *w, const double *s,
                   float2 *U, double *part, int width)
 {
+    if (v == kTmVariant) {
+        launch_tm(c, st, w, s, U, part, width);
+        return;
+    }
     if (v >= kNumSimtVariants) {
         launch_tc(c, tc_cube_bits(v), st, w, s, U, part, width);
         return;
@@ -1718,7 +1771,7 @@ int tune_quartet_tile(msgpu_ctx *c, const float2 *w, const double *s, float2 *U,
     size_t smem;
     for (int v = 0; v < kNumSpmmVariants; ++v) {
         if (c->spmm_variant >= 0 && v != c->spmm_variant) continue;
-        if (c->spmm_variant < 0 && v >= kNumSimtVariants && !kTcInTuner) continue;
+        if (c->spmm_variant < 0 && !in_tuner(v)) continue;
         for (int qt : cand)
             if ((qt <= Q || qt == cand[0]) && apply_fits(c, v, qt, &smem)) cands.push_back({v, qt});
     }
@@ -2410,7 +2463,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
     collect_profile(c);
     c->last_ntimes = p->ntimes;
     c->have_integrals = true;
-    if (status & 4) return fail(c, MSGPU_ERR_CUDA, "run: tensor-core SpMM pipeline timed out (bounded wait expired)");
+    if (status & 4) return fail(c, MSGPU_ERR_CUDA, "run: tensor-core or TMEM-staged SpMM pipeline timed out (bounded wait expired)");
     if (status & 2) return fail(c, MSGPU_ERR_NONFINITE, "run: non-finite observable or norm on the device");
     if (status & 1) return fail(c, MSGPU_ERR_EXPM, "run: small matrix exponential failed");
     return MSGPU_OK;

@@ -540,8 +540,19 @@ __device__ __forceinline__ void mac_pp(float2 o[2], float br_, float bi_, float4
     o[1] = __ffma2_rn(bi, re, o[1]);
 }
 
+// Load of a block value: read-only global path, or a plain load (values
+// staged in shared memory).
+template <bool kGlobal>
+__device__ __forceinline__ float4 qb_ld(const float4 *v)
+{
+    if constexpr (kGlobal) return __ldg(v);
+    else return *v;
+}
+
 // o[a] = {re pair, im pair} of output row a; v = the block's values, two
-// complex values per float4 in the storage order of the type.
+// complex values per float4 in the storage order of the type (in global
+// memory, or with kGlobal = false anywhere a plain load reaches).
+template <bool kGlobal = true>
 __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const float4 *__restrict__ v,
                                               const float4 x[4])
 {
@@ -549,7 +560,7 @@ __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const fl
     case 0:
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const float4 p = __ldg(v + 2 * a), q = __ldg(v + 2 * a + 1);
+            const float4 p = qb_ld<kGlobal>(v + 2 * a), q = qb_ld<kGlobal>(v + 2 * a + 1);
             mac_pp(o[a], p.x, p.y, x[0]);
             mac_pp(o[a], p.z, p.w, x[1]);
             mac_pp(o[a], q.x, q.y, x[2]);
@@ -561,7 +572,7 @@ __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const fl
         for (int a2 = 0; a2 < 2; ++a2)
 #pragma unroll
             for (int a1 = 0; a1 < 2; ++a1) {
-                const float4 p = __ldg(v + 2 * a2 + a1);
+                const float4 p = qb_ld<kGlobal>(v + 2 * a2 + a1);
                 mac_pp(o[2 * a1 + a2], p.x, p.y, x[a2]);
                 mac_pp(o[2 * a1 + a2], p.z, p.w, x[2 + a2]);
             }
@@ -571,13 +582,13 @@ __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const fl
         for (int a1 = 0; a1 < 2; ++a1)
 #pragma unroll
             for (int a2 = 0; a2 < 2; ++a2) {
-                const float4 p = __ldg(v + 2 * a1 + a2);
+                const float4 p = qb_ld<kGlobal>(v + 2 * a1 + a2);
                 mac_pp(o[2 * a1 + a2], p.x, p.y, x[2 * a1]);
                 mac_pp(o[2 * a1 + a2], p.z, p.w, x[2 * a1 + 1]);
             }
         break;
     case 3: {
-        const float4 p = __ldg(v), q = __ldg(v + 1);
+        const float4 p = qb_ld<kGlobal>(v), q = qb_ld<kGlobal>(v + 1);
         mac_pp(o[0], p.x, p.y, x[0]);
         mac_pp(o[1], p.z, p.w, x[1]);
         mac_pp(o[2], q.x, q.y, x[2]);
@@ -585,7 +596,7 @@ __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const fl
         break;
     }
     case 4: {
-        const float4 p = __ldg(v), q = __ldg(v + 1);  // A00 A01 | A10 A11
+        const float4 p = qb_ld<kGlobal>(v), q = qb_ld<kGlobal>(v + 1);  // A00 A01 | A10 A11
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2) {
             mac_pp(o[a2], p.x, p.y, x[a2]);
@@ -596,7 +607,7 @@ __device__ __forceinline__ void quartet_block(float2 o[4][2], int type, const fl
         break;
     }
     default: {
-        const float4 p = __ldg(v), q = __ldg(v + 1);
+        const float4 p = qb_ld<kGlobal>(v), q = qb_ld<kGlobal>(v + 1);
 #pragma unroll
         for (int a1 = 0; a1 < 2; ++a1) {
             mac_pp(o[2 * a1], p.x, p.y, x[2 * a1]);

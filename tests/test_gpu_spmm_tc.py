@@ -1,12 +1,17 @@
-"""GPU: the tensor-core quartet SpMM of the complex64 Lanczos form
-(k_lanczos_apply_tc, SpMM variants 8 and 9: cubes of 16 and 8 output quartets)
-against the SIMT quartet SpMM, the complex128 path and the oracle.
+"""GPU: the cube-blocked quartet SpMMs of the complex64 Lanczos form against
+the SIMT quartet SpMM, the complex128 path and the oracle:
+- the tensor-core SpMM (k_lanczos_apply_tc, variants 8 and 9: cubes of 16 and
+  8 output quartets);
+- the TMEM-staged SpMM (k_lanczos_apply_tm, variant 10: persistent CTAs over
+  cubes of 8 quartets x 256 trajectories, inputs through TMA, tcgen05.cp and
+  tcgen05.ld, FP32 block arithmetic).
 
-Both complex64 SpMMs apply the same FP32 quartet blocks; the tensor-core one
+All complex64 SpMMs apply the same FP32 quartet blocks; the tensor-core one
 splits inputs and blocks into a TF32 head and an FP32 tail and accumulates in
-FP32 in tensor memory (dropped products 2^-22 of the result), so yields of the
-two complex64 forms agree to FP32 rounding carried through the run and both
-stay within the precision form's 1e-6 (relative, per trajectory) of complex128.
+FP32 in tensor memory (dropped products 2^-22 of the result), the TMEM-staged
+one sums the same products as the SIMT kernels in another order. Yields of the
+complex64 forms agree to FP32 rounding carried through the run and all stay
+within the precision form's 1e-6 (relative, per trajectory) of complex128.
 """
 import numpy as np
 import pytest
@@ -20,6 +25,8 @@ from tests import helpers as h
 pytestmark = pytest.mark.gpu
 
 TC_VARIANTS = [8, 9]   # cube bits 4, 3
+TM_VARIANT = 10        # TMEM-staged, cube bits 3
+CUBE_VARIANTS = TC_VARIANTS + [TM_VARIANT]
 SIMT_VARIANT = 7       # k_lanczos_apply_np<2, 3>
 
 
@@ -48,7 +55,7 @@ def _run(system, F, times, precision, variant=None, noise=None, krylov=16):
         return per, ens, p.values(), napply
 
 
-@pytest.mark.parametrize("variant", TC_VARIANTS)
+@pytest.mark.parametrize("variant", CUBE_VARIANTS)
 def test_tc_against_simt_and_complex128(variant):
     # D = 1024 (P = 8 quartet bits), anisotropic couplings, Philox dephasing,
     # 200 trajectories (a padded block: the last 56 columns of the tile are zero)
@@ -81,7 +88,7 @@ def _interleaved(second: int):
     return s, rng
 
 
-@pytest.mark.parametrize("variant", TC_VARIANTS)
+@pytest.mark.parametrize("variant", CUBE_VARIANTS)
 def test_tc_interleaved_electrons_small_tile_against_oracle(variant):
     # electrons at basis positions 1 and 3 (strides 64 and 16: a cube's quartets
     # still have consecutive rows), 64 trajectories: one half-filled 128-trajectory tile
@@ -96,13 +103,14 @@ def test_tc_interleaved_electrons_small_tile_against_oracle(variant):
     assert _rel(val_t, ref["values"]) < 1e-6
 
 
-def test_tc_precision_configuration_two_groups():
+@pytest.mark.parametrize("variant", [8, TM_VARIANT])
+def test_tc_precision_configuration_two_groups(variant):
     # D = 16384 (P = 12), 512 trajectories: two trajectory groups of 256 on two
     # streams; 100 steps against the SIMT SpMM and complex128
     w = S.precision_large(M=512, steps=100)
     F = w.system.trace_samples(w.M, w.seed)
     times = w.times()
-    per_t, ens_t, val_t, _ = _run(w.system, F, times, "c64", 8, krylov=w.krylov)
+    per_t, ens_t, val_t, _ = _run(w.system, F, times, "c64", variant, krylov=w.krylov)
     per_s, _, _, _ = _run(w.system, F, times, "c64", SIMT_VARIANT, krylov=w.krylov)
     per_d, ens_d, val_d, _ = _run(w.system, F, times, "c128", krylov=w.krylov)
     assert _rel(per_t, per_s) < 1e-6
@@ -111,7 +119,8 @@ def test_tc_precision_configuration_two_groups():
     assert _rel(val_t, val_d) < 1e-6
 
 
-def test_tc_tables_follow_field_terms():
+@pytest.mark.parametrize("variant", [8, TM_VARIANT])
+def test_tc_tables_follow_field_terms(variant):
     # H = H_0 + Bx Zx + By Zy + Bz Zz: a field change through the coefficients
     # refreshes the tensor-core tables on the device; the result equals the
     # complex128 path of a context built for the new field
@@ -131,7 +140,7 @@ def test_tc_tables_follow_field_terms():
     F = s1.trace_samples(M, 2.0)
     with hs.HSPropagatorB200(0) as p:
         p.set_form("streamed")
-        p.set_option(L.OPT_SPMM_VARIANT, 8)
+        p.set_option(L.OPT_SPMM_VARIANT, variant)
         p.set_hamiltonian_terms(r, c, v, [1.0, *B1])
         p.set_reaction(kappa=s1.kappa())
         p.set_electron_pair(*s1.electron_strides())
@@ -149,13 +158,32 @@ def test_tc_tables_follow_field_terms():
     assert _rel(per1, per2) > 1e-4
 
 
-def test_tc_refused_without_the_nuclear_bit_structure():
-    # a spin-1 nucleus: quartets are not bit-indexed, so the forced tensor-core
+def test_tm_second_electron_stride_of_one_cube_against_oracle():
+    # electrons at positions 1 and 4: the second stride is 8, one 8-quartet cube,
+    # so the TMEM-staged SpMM's boxes still load whole cubes; 320 trajectories:
+    # a full and a partly filled 256-trajectory tile
+    s, rng = _interleaved(4)
+    M, times = 320, S.time_grid(30.0, 1.0)
+    F = rng.normal(size=(s.dim, M)) + 1j * rng.normal(size=(s.dim, M))
+    F /= np.linalg.norm(F, axis=0) * np.sqrt(M)
+    per_t, _, val_t, _ = _run(s, F, times, "c64", TM_VARIANT, krylov=12)
+    ref = orc.hs_stochastic(s.hamiltonian_csr(), F, times, h.oracle_observables(s), kappa=s.kappa(), krylov=12,
+                            nthreads=8)
+    assert _rel(per_t, ref["traj_yield"]) < 1e-6
+    assert _rel(val_t, ref["values"]) < 1e-6
+
+
+@pytest.mark.parametrize("variant", CUBE_VARIANTS)
+def test_tc_refused_without_the_nuclear_bit_structure(variant):
+    # a spin-1 nucleus: quartets are not bit-indexed, so the forced cube-blocked
     # variant is refused with an error rather than run
     s = h.random_system([2, 3], [2], seed=3)
     F = s.trace_samples(64, 1.0)
     with pytest.raises(hs.MsgpuError):
-        _run(s, F, S.time_grid(4.0, 1.0), "c64", 8)
+        _run(s, F, S.time_grid(4.0, 1.0), "c64", variant)
+
+
+def test_tc_refused_when_a_cube_is_not_consecutive_rows():
     # electrons at positions 1 and 4: the second stride is 8, so a 16-quartet
     # cube's rows are not consecutive and variant 8's boxes cannot load it
     s, rng = _interleaved(4)
