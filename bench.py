@@ -50,6 +50,8 @@ def _args():
                          "tensor-core propagator; batching: 64 uneven systems; serving: a request stream")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=4.0, help="serving: Poisson arrival rate (requests/s)")
+    ap.add_argument("--pack-dim", type=int, default=2048,
+                    help="serving: requests below this dimension share batch launches (0: one context each)")
     ap.add_argument("--precision", default=None, help="dense: bf16x3 | bf16x6 | int8x4")
     ap.add_argument("--spmm-variant", type=int, default=-1,
                     help="precision form: -1 autotuned SpMM variant (default), k >= 0 force variant k")
@@ -688,7 +690,8 @@ def run_serving(args):
     arr = SV.poisson_arrivals(args.requests, args.rate, seed=5 + rank)
     reqs = [SV.Request(i, float(arr[i]), S.serving_request(i + 100000 * rank, grid), seed=7000 + i)
             for i in range(args.requests)]
-    eng = SV.ServingEngine(local, hbm_budget=120 << 30, slots=8)
+    pack_dim = getattr(args, "pack_dim", 2048)
+    eng = SV.ServingEngine(local, hbm_budget=120 << 30, slots=8, pack_dim=pack_dim)
     clocks = ClockSampler(local)
     clocks.start()
     _barrier(world)
@@ -711,10 +714,11 @@ def run_serving(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP64 reductions/expm/sums)",
         "data": "synthetic (seeded)",
         "config": {"workload": f"{args.requests} requests, Poisson {args.rate}/s, 6-14 nuclei, M=256, 3000 steps",
-                   "slots": 8, "hbm_budget_gib": 120},
+                   "slots": 8, "hbm_budget_gib": 120, "pack_dim": pack_dim},
         "latency_s": {"p50": s["p50_latency_s"], "p99": s["p99_latency_s"], "mean": s["mean_latency_s"]},
         "completed": s["completed"], "failed": s["failed"], "max_concurrency": eng.max_concurrency,
         "contexts": {"created": eng.contexts_created, "reused": eng.contexts_reused},
+        "packs": {"launches": eng.packs, "requests": eng.packed},
         "peak_reserved_gib": eng.peak_reserved / 2 ** 30,
         "roofline": {"bound": "hbm", "kernel": "whole stream ((4m+1) D c bytes per traj-step)", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,

@@ -301,6 +301,14 @@ const char *msgpu_batch_last_error(const msgpu_batch *batch);
 int msgpu_batch_add_system(msgpu_batch *batch, int dim, const int *rowptr, const int *col, const double *val,
                            double kappa, int stride1, int stride2, int nobs, const double *ops, const double *rates,
                            double st_rate, unsigned long long seed, int ntraj, const double *factors);
+/* Drops every system of the batch (the team threshold and CTAs per SM of a
+ * previous tune stay).  The device buffers of persistent-route systems are
+ * kept and serve the next msgpu_batch_add_system calls, so a pooled batch
+ * runs one group of systems after another without allocating or freeing
+ * device memory; a streamed system's context is destroyed.  Waits for the
+ * batch's stream.  Replaces nothing in the reference: its orientation and
+ * RunSection loops hold no device state. */
+int msgpu_batch_clear(msgpu_batch *batch);
 int msgpu_batch_tune(msgpu_batch *batch, const double *times, int ntimes, int krylov_dim);
 int msgpu_batch_run(msgpu_batch *batch, const double *times, int ntimes, int krylov_dim, long long step_offset,
                     int accumulate);

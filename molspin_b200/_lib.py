@@ -107,6 +107,7 @@ def _load() -> C.CDLL:
         "msgpu_get_option": (I, [P, I, pD]),
         "msgpu_batch_create": (P, [I, C.c_size_t]),
         "msgpu_batch_destroy": (None, [P]),
+        "msgpu_batch_clear": (I, [P]),
         "msgpu_batch_last_error": (C.c_char_p, [P]),
         "msgpu_batch_add_system": (I, [P, I, pI, pI, pD, D, I, I, I, pD, pD, D, C.c_ulonglong, I, pD]),
         "msgpu_batch_tune": (I, [P, pD, I, I]),

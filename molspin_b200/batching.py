@@ -72,6 +72,12 @@ class BatchB200:
         self.systems.append((M, len(obs)))
         return idx
 
+    def clear(self):
+        """Drops every system; the device buffers of the persistent route are
+        kept for the next add() calls (msgpu_batch_clear)."""
+        self._check(L.lib.msgpu_batch_clear(self.b))
+        self.systems.clear()
+
     def tune(self, times: np.ndarray, krylov: int):
         t = np.ascontiguousarray(times, np.float64)
         self._check(L.lib.msgpu_batch_tune(self.b, L.dptr(t), len(t), int(krylov)))

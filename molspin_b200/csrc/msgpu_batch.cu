@@ -54,6 +54,9 @@ struct msgpu_batch {
     cudaStream_t stream = nullptr;
     std::string err;
     std::vector<BatchSystem> sys;
+    // systems of the persistent route dropped by msgpu_batch_clear: their device
+    // buffers serve the next msgpu_batch_add_system (no cudaMalloc / cudaFree per reuse)
+    std::vector<BatchSystem> spare;
     Buf sys_d, items_d, queue_d, status_d, scratch, times_d, backup;
     int threshold = 512, ctas_per_sm = 2, tuned = 0;
     int sm_count = 0;
@@ -332,11 +335,12 @@ void msgpu_batch_destroy(msgpu_batch *b)
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
     drop_graph(b);
-    for (auto &s : b->sys) {
-        Buf *all[] = {&s.rowptr, &s.col, &s.valf, &s.obs, &s.rates, &s.psi, &s.acc, &s.comp, &s.prev, &s.pflip};
-        for (Buf *x : all) brelease(b, *x);
-        if (s.ctx) msgpu_destroy(s.ctx);
-    }
+    for (auto *list : {&b->sys, &b->spare})
+        for (auto &s : *list) {
+            Buf *all[] = {&s.rowptr, &s.col, &s.valf, &s.obs, &s.rates, &s.psi, &s.acc, &s.comp, &s.prev, &s.pflip};
+            for (Buf *x : all) brelease(b, *x);
+            if (s.ctx) msgpu_destroy(s.ctx);
+        }
     Buf *all[] = {&b->sys_d, &b->items_d, &b->queue_d, &b->status_d, &b->scratch, &b->times_d, &b->backup};
     for (Buf *x : all) brelease(b, *x);
     cudaStreamDestroy(b->stream);
@@ -344,6 +348,25 @@ void msgpu_batch_destroy(msgpu_batch *b)
 }
 
 const char *msgpu_batch_last_error(const msgpu_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int msgpu_batch_clear(msgpu_batch *b)
+{
+    if (!b) return MSGPU_ERR_INVALID;
+    cudaSetDevice(b->device);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, MSGPU_ERR_CUDA, "batch: clear: stream failed");
+    drop_graph(b);
+    for (auto &s : b->sys) {
+        if (s.ctx) {
+            msgpu_destroy(s.ctx);  // a streamed system's context goes with it
+            s.ctx = nullptr;
+        } else {
+            b->spare.push_back(s);
+        }
+    }
+    b->sys.clear();
+    b->tuned = 0;
+    return MSGPU_OK;
+}
 
 int msgpu_batch_add_system(msgpu_batch *b, int dim, const int *rowptr, const int *col, const double *val,
                            double kappa, int stride1, int stride2, int nobs, const double *ops, const double *rates,
@@ -392,6 +415,10 @@ int msgpu_batch_add_system(msgpu_batch *b, int dim, const int *rowptr, const int
         return static_cast<int>(b->sys.size()) - 1;
     }
     BatchSystem s;
+    if (!b->spare.empty()) {  // reuse a cleared system's buffers (upload keeps those large enough)
+        s = b->spare.back();
+        b->spare.pop_back();
+    }
     s.D = dim;
     s.M = ntraj;
     s.nobs = nobs;
@@ -431,9 +458,14 @@ int msgpu_batch_add_system(msgpu_batch *b, int dim, const int *rowptr, const int
         (rc = upload(b, s.psi, psi.data(), sizeof(float) * psi.size(), "factors")) ||
         (rc = upload(b, s.acc, zeros.data(), sizeof(double) * zeros.size(), "acc")) ||
         (rc = upload(b, s.comp, zeros.data(), sizeof(double) * zeros.size(), "comp")) ||
-        (rc = upload(b, s.prev, zeros.data(), sizeof(double) * zeros.size(), "prev")))
+        (rc = upload(b, s.prev, zeros.data(), sizeof(double) * zeros.size(), "prev"))) {
+        b->spare.push_back(s);  // its buffers are freed with the batch
         return -rc;
-    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return -bfail(b, MSGPU_ERR_CUDA, "batch: upload failed");
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        b->spare.push_back(s);
+        return -bfail(b, MSGPU_ERR_CUDA, "batch: upload failed");
+    }
     b->sys.push_back(s);
     drop_graph(b);
     b->tuned = 0;

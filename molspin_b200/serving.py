@@ -19,6 +19,15 @@ the whole device, i.e. for every other request's kernels).  Idle contexts
 keep their reservation and are destroyed only when an admission needs the
 memory.
 
+Small systems share launches.  Requests below `pack_dim` (the batching
+form's persistent route, D < 2048) that share a time grid and Krylov
+dimension are admitted together, up to `pack_max` of them in one slot, and
+run as one persistent launch of the batching form (msgpu_batch_*) on a
+pooled batch whose device buffers are kept between packs
+(msgpu_batch_clear).  A system's result in a batch does not depend on its
+companions, and a small request solved alone also runs as a one-system
+batch, so a packed result equals its solo run bit for bit.
+
 Results do not depend on the mix: noise is counter-based Philox keyed by the
 request's seed and each trajectory/step, reductions are two-phase in a fixed
 order, and the SpMM tile chosen by the autotuner only changes how partial
@@ -83,15 +92,22 @@ def footprint(w: Workload, precision: str = "c64") -> int:
 
 
 class ServingEngine:
-    def __init__(self, device: int = 0, hbm_budget: int = 64 << 30, slots: int = 8, precision: str = "c64"):
+    def __init__(self, device: int = 0, hbm_budget: int = 64 << 30, slots: int = 8, precision: str = "c64",
+                 pack_dim: int = 2048, pack_max: int = 16):
         self.device = device
         self.budget = hbm_budget
         self.slots = slots
         self.precision = precision
+        self.pack_dim = pack_dim    # requests below this dimension are packed (0: never)
+        self.pack_max = pack_max    # requests per pack
         self._lock = threading.Condition()
         self._reserved = 0   # running requests plus idle pooled contexts
-        self._running = 0
+        self._running = 0    # slots in use (a pack takes one)
+        self._inflight = 0   # requests running
         self._idle: dict[tuple, list[tuple[HSPropagatorB200, int]]] = {}  # shape -> [(context, reserved)]
+        self._idle_batches: list[tuple[object, int]] = []                 # [(pooled batch, reserved)]
+        self.packs = 0
+        self.packed = 0
         self.max_concurrency = 0
         self.peak_reserved = 0
         self.contexts_created = 0
@@ -100,6 +116,14 @@ class ServingEngine:
     @staticmethod
     def shape(w: Workload) -> tuple:
         return (w.system.dim, w.M, w.krylov, w.steps)
+
+    def packable(self, w: Workload) -> bool:
+        return self.precision == "c64" and 0 < w.system.dim < self.pack_dim
+
+    @staticmethod
+    def pack_key(w: Workload) -> tuple:
+        """Requests of one pack share the time grid and the Krylov dimension."""
+        return (w.steps, w.dt, w.krylov)
 
     def _run(self, p: HSPropagatorB200, req: Request) -> np.ndarray:
         w = req.workload
@@ -120,10 +144,33 @@ class ServingEngine:
         return ens
 
     def solve(self, req: Request, budget: int = 0) -> np.ndarray:
-        """One request on a context of its own (created and destroyed here);
-        returns the ensemble yields."""
+        """One request on a context of its own (created and destroyed here;
+        a one-system batch when it would be packed); returns the ensemble yields."""
+        if self.packable(req.workload):
+            ens, batch = self.solve_pack([req], None)
+            batch.close()
+            return ens[0]
         with HSPropagatorB200(self.device, budget) as p:
             return self._run(p, req)
+
+    def solve_pack(self, reqs: list[Request], batch):
+        """Requests of one pack key in one persistent launch on a pooled batch
+        (a new one when batch is None); returns (ensemble yields per request,
+        the batch to keep for the pool)."""
+        from .batching import BatchB200
+        if batch is None:
+            batch = BatchB200(self.device)
+        try:
+            batch.clear()
+            for q in reqs:
+                w = q.workload
+                batch.add(w.system, w.system.trace_samples(w.M, w.seed), q.seed)
+            w0 = reqs[0].workload
+            batch.run(w0.times(), w0.krylov)
+            return [batch.yields(i)[1] for i in range(len(reqs))], batch
+        except Exception:
+            batch.close()
+            raise
 
     def solve_pooled(self, req: Request, budget: int, ctx):
         """One request on a pooled context (a new one when ctx is None);
@@ -149,7 +196,74 @@ class ServingEngine:
             else:
                 self._reserved -= res.reserved
             self._running -= 1
+            self._inflight -= 1
             self._lock.notify_all()
+
+    def _pack_worker(self, reqs: list[Request], ress: list[Result], t0: float, batch, reserved: int):
+        try:
+            ens, batch = self.solve_pack(reqs, batch)
+            for r, e in zip(ress, ens):
+                r.yields = e
+        except Exception as e:  # noqa: BLE001 -- reported per request
+            for r in ress:
+                r.error = str(e)
+            batch = None
+        fin = time.perf_counter() - t0
+        for r in ress:
+            r.finished = fin
+        with self._lock:
+            if batch is not None:
+                self._idle_batches.append((batch, reserved))
+            else:
+                self._reserved -= reserved
+            self._running -= 1
+            self._inflight -= len(reqs)
+            self._lock.notify_all()
+
+    def _admit_pack(self, first: Request, waiting: list[Request], results: dict, now: float, t0: float,
+                    threads: list) -> bool:
+        """Admits `first` with the waiting requests of its pack key (called with
+        the lock held and a slot free); False when not even `first` fits."""
+        key = self.pack_key(first.workload)
+        group = [q for q in waiting if self.packable(q.workload) and self.pack_key(q.workload) == key]
+        group = group[:self.pack_max]
+        batch, held = self._idle_batches.pop() if self._idle_batches else (None, 0)
+        need = lambda g: max(held, sum(results[q.rid].reserved for q in g)) - held  # noqa: E731
+        if self._reserved + need(group) > self.budget:
+            evicted = self._evict(need(group))
+            if evicted:
+                self._lock.release()
+                try:
+                    for c, _ in evicted:
+                        c.close()
+                finally:
+                    self._lock.acquire()
+        while group and self._reserved + need(group) > self.budget:
+            group.pop()
+        if not group:
+            if batch is not None:
+                self._idle_batches.append((batch, held))
+            return False
+        extra = need(group)
+        self._reserved += extra
+        if batch is None:
+            self.contexts_created += 1
+        else:
+            self.contexts_reused += 1
+        for q in group:
+            waiting.remove(q)
+            results[q.rid].admitted = now
+        self._running += 1
+        self._inflight += len(group)
+        self.packs += 1
+        self.packed += len(group)
+        self.max_concurrency = max(self.max_concurrency, self._inflight)
+        self.peak_reserved = max(self.peak_reserved, self._reserved)
+        th = threading.Thread(target=self._pack_worker,
+                              args=(group, [results[q.rid] for q in group], t0, batch, held + extra), daemon=True)
+        th.start()
+        threads.append(th)
+        return True
 
     def _evict(self, need: int) -> list[tuple[HSPropagatorB200, int]]:
         """Idle contexts to destroy (largest first) so that `need` more bytes fit;
@@ -172,10 +286,11 @@ class ServingEngine:
         return out
 
     def close(self):
-        """Destroys the idle pooled contexts."""
+        """Destroys the idle pooled contexts and batches."""
         with self._lock:
-            idle = [c for lst in self._idle.values() for c in lst]
+            idle = [c for lst in self._idle.values() for c in lst] + self._idle_batches
             self._idle.clear()
+            self._idle_batches = []
             self._reserved -= sum(r for _, r in idle)
         for ctx, _ in idle:
             ctx.close()
@@ -207,6 +322,10 @@ class ServingEngine:
                 while k < len(waiting) and self._running < self.slots:
                     req = waiting[k]
                     res = results[req.rid]
+                    if self.packable(req.workload):
+                        if not self._admit_pack(req, waiting, results, now, t0, threads):
+                            k += 1
+                        continue
                     ctx = None
                     pooled = self._idle.get(self.shape(req.workload))
                     if pooled:
@@ -229,7 +348,8 @@ class ServingEngine:
                         self.contexts_created += 1
                     waiting.pop(k)
                     self._running += 1
-                    self.max_concurrency = max(self.max_concurrency, self._running)
+                    self._inflight += 1
+                    self.max_concurrency = max(self.max_concurrency, self._inflight)
                     self.peak_reserved = max(self.peak_reserved, self._reserved)
                     res.admitted = now
                     th = threading.Thread(target=self._worker, args=(req, res, t0, ctx), daemon=True)

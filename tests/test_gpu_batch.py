@@ -68,6 +68,25 @@ def test_batch_result_independent_of_companions_and_chunks():
         np.testing.assert_array_equal(x[0], y[0])
 
 
+def test_cleared_batch_reuses_its_buffers_and_matches_fresh_batches():
+    # a batch cleared between groups of systems (msgpu_batch_clear keeps the
+    # persistent route's device buffers) gives each group the result of a
+    # fresh batch, bit for bit, including a group smaller than the first
+    entries = _systems()
+    times = S.time_grid(20.0, 1.0)
+    fresh_all, _ = _run(entries, times, 10)
+    fresh_one, _ = _run(entries[1:2], times, 10)
+    with B.BatchB200(0) as bt:
+        for group, ref in ((entries, fresh_all), (entries[1:2], fresh_one), (entries, fresh_all)):
+            bt.clear()
+            idx = [bt.add(s, s.trace_samples(M, float(seed)), seed) for s, M, seed in group]
+            bt.run(times, 10)
+            for i, (per, ens) in zip(idx, ref):
+                got = bt.yields(i)
+                np.testing.assert_array_equal(got[0], per)
+                np.testing.assert_array_equal(got[1], ens)
+
+
 def test_batch_streams_large_systems_through_the_single_system_path():
     # D = 2048 reaches the streamed threshold: it runs on its own context
     # beside the persistent launch, and equals the single-system complex64 run

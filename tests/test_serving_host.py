@@ -1,6 +1,6 @@
 """Host logic of the serving engine without a GPU: admission against slots
-and the memory budget, first-fit order, arrival times, the context pool and
-the summary."""
+and the memory budget, first-fit order, arrival times, the context pool,
+packing of small requests into shared batch launches, and the summary."""
 import threading
 import time
 
@@ -22,7 +22,9 @@ class FakeCtx:
 
 
 class FakeEngine(SV.ServingEngine):
+    """Per-request contexts only (packing off unless asked for)."""
     def __init__(self, *a, work_s=0.05, **k):
+        k.setdefault("pack_dim", 0)
         super().__init__(*a, **k)
         self.work_s = work_s
         self.active = 0
@@ -125,3 +127,80 @@ def test_idle_contexts_are_evicted_when_memory_is_needed():
     assert all(not r.error for r in res), [r.error for r in res]
     assert eng.peak_reserved <= eng.budget
     assert eng.ctxs[0].closed and eng.contexts_created == 2
+
+
+class FakeBatch:
+    def __init__(self):
+        self.closed = False
+        self.runs = 0
+
+    def close(self):
+        self.closed = True
+
+
+class FakePackEngine(FakeEngine):
+    """Packing on: solve_pack records each pack instead of launching it."""
+    def __init__(self, *a, **k):
+        k.setdefault("pack_dim", 2048)
+        super().__init__(*a, **k)
+        self.packs_seen = []
+        self.batches = []
+
+    def solve_pack(self, reqs, batch):
+        with self.lock:
+            if batch is None:
+                batch = FakeBatch()
+                self.batches.append(batch)
+            assert not batch.closed
+            batch.runs += 1
+            self.packs_seen.append([q.rid for q in reqs])
+        time.sleep(self.work_s)
+        return [np.array([float(q.rid)]) for q in reqs], batch
+
+
+def _small(i, steps=10, arrival=0.0):
+    return SV.Request(i, arrival, S.serving_request(i, nuclei=(6, 7), steps=steps), seed=i)
+
+
+def test_small_requests_share_pack_launches():
+    # ten small requests at once through two slots, at most four per pack: every
+    # request completes with its own result, in packs of one key, on pooled batches
+    reqs = [_small(i) for i in range(10)]
+    eng = FakePackEngine(hbm_budget=1 << 40, slots=2, pack_max=4, work_s=0.02)
+    res = eng.serve(reqs, realtime=False)
+    assert all(not r.error for r in res)
+    assert [r.yields[0] for r in res] == list(range(10))
+    assert sorted(i for p in eng.packs_seen for i in p) == list(range(10))
+    assert all(len(p) <= 4 for p in eng.packs_seen) and len(eng.packs_seen) >= 3
+    assert eng.packs == len(eng.packs_seen) and eng.packed == 10
+    assert len(eng.batches) <= 2 and all(b.closed for b in eng.batches)
+    assert eng.ctxs == [] and eng._reserved == 0
+    assert eng.max_concurrency <= 2 * 4
+
+
+def test_packs_hold_one_time_grid_and_large_requests_keep_their_contexts():
+    # two step counts (two time grids) and one system above the packing
+    # dimension: packs never mix grids; the large request runs on a context
+    reqs = [_small(i, steps=10 if i % 2 else 20) for i in range(6)]
+    reqs.append(SV.Request(6, 0.0, S.serving_request(6, nuclei=(9, 9), steps=10), seed=6))  # D = 2048
+    eng = FakePackEngine(hbm_budget=1 << 40, slots=4, work_s=0.01)
+    res = eng.serve(reqs, realtime=False)
+    assert all(not r.error for r in res)
+    steps = {q.rid: q.workload.steps for q in reqs}
+    for p in eng.packs_seen:
+        assert len({steps[i] for i in p}) == 1
+    assert 6 not in {i for p in eng.packs_seen for i in p}
+    assert sum(c.served for c in eng.ctxs) == 1 and eng.started == [6]
+
+
+def test_packs_shrink_to_the_budget():
+    # a budget of three of the largest footprints, below four of the smallest:
+    # no pack holds more than three
+    reqs = [_small(i) for i in range(7)]
+    sizes = [SV.footprint(q.workload) for q in reqs]
+    assert 4 * min(sizes) > 3 * max(sizes)
+    eng = FakePackEngine(hbm_budget=3 * max(sizes), slots=4, work_s=0.01)
+    res = eng.serve(reqs, realtime=False)
+    assert all(not r.error for r in res)
+    assert eng.peak_reserved <= eng.budget
+    assert all(len(p) <= 3 for p in eng.packs_seen)
