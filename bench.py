@@ -255,6 +255,7 @@ def run_ours(args):
     el_ms = ev0.elapsed_time(ev1)
     apply_ms, apply_n = p.profile_read(L.KC_APPLY)
     orth_ms, orth_n = p.profile_read(L.KC_ORTH)
+    red_ms, red_n = p.profile_read(L.KC_REDUCE)
     comb_ms, comb_n = p.profile_read(L.KC_COMBINE)
     fused_ms, fused_n = p.profile_read(L.KC_LANCZOS)
     p.profile(False)
@@ -366,6 +367,7 @@ def run_ours(args):
                               "split_kernel_bytes_per_time_step": step_bytes_split,
                               "split_kernel_frac": step_bytes_split / step_s / 1e9 / hbm_peak},
             "kernel_avg_ms": {"apply": apply_ms / max(1, apply_n), "update": orth_ms / max(1, orth_n),
+                              "reduce": red_ms / max(1, red_n),
                               "combine": comb_ms / max(1, comb_n),
                               **({"lanczos_cluster_resident": fused_ms / fused_n} if fused_n else {})},
             "lanczos": "cluster-resident recurrence" if fused_n else "SpMM + update + reductions per iteration",

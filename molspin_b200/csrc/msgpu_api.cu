@@ -2412,7 +2412,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                     }
                     {
                         Timed tm(c, KC_REDUCE, gs);
-                        k_lanczos_reduce<<<width / 32, dim3(32, 8), 0, gs>>>(part + t0, nqt, ldm, 0, j, mws, alpha + t0,
+                        k_lanczos_reduce<<<width / 32, dim3(32, kRedRows), 0, gs>>>(part + t0, nqt, ldm, 0, j, mws, alpha + t0,
                                                                              td + tm0, to + tm0, mdim + t0);
                     }
                     if (j == m - 1) break;  // T_m is complete; w_m is never used
@@ -2425,7 +2425,7 @@ int msgpu_run(msgpu_ctx *c, const msgpu_run_params *p)
                     }
                     {
                         Timed tm(c, KC_REDUCE, gs);
-                        k_lanczos_reduce<<<width / 32, dim3(32, 8), 0, gs>>>(part + t0, nt, ldm, 1, j, mws,
+                        k_lanczos_reduce<<<width / 32, dim3(32, kRedRows), 0, gs>>>(part + t0, nt, ldm, 1, j, mws,
                                                                              sc + static_cast<size_t>(j + 1) * ldm + t0,
                                                                              td + tm0, to + tm0, mdim + t0);
                     }

@@ -977,22 +977,26 @@ k_lanczos_update(const float2 *__restrict__ U, const float2 *__restrict__ wj, co
 // out[t] = sum over tiles of part[tile][t] (fixed order), optional sqrt and
 // Lanczos bookkeeping: mode 0 -> alpha_j (stored to T diag), mode 1 -> beta_{j+1}
 // (stored to T offdiag, scale = 1/beta, breakdown marks the dimension).
-// Launch with blockDim (32, 8) and ldm/32 blocks: thread (x, y) sums tiles
-// y, y+8, ... of trajectory t, then the 8 column sums are added in order.
-__global__ void k_lanczos_reduce(const double *__restrict__ part, int ntiles, int ldm, int mode, int j, int m,
-                                 double *__restrict__ out, double *__restrict__ tdiag, double *__restrict__ toff,
-                                 int *__restrict__ mdim)
+// Launch with blockDim (32, kRedRows) and ldm/32 blocks: thread (x, y) sums
+// tiles y, y + kRedRows, ... of trajectory t, then the kRedRows column sums
+// are added in order.  A group of 512 trajectories gives only 16 CTAs, so each
+// thread's chain of dependent L2 loads sets the time: 32 rows keep it at
+// 8 loads for the 256 tile partials of the SpMM.
+constexpr int kRedRows = 32;
+__global__ void __launch_bounds__(32 * kRedRows)
+k_lanczos_reduce(const double *__restrict__ part, int ntiles, int ldm, int mode, int j, int m, double *__restrict__ out,
+                 double *__restrict__ tdiag, double *__restrict__ toff, int *__restrict__ mdim)
 {
-    __shared__ double red[8][33];
+    __shared__ double red[kRedRows][33];
     const int t = blockIdx.x * 32 + threadIdx.x;
     double ps = 0.0;
-    for (int tile = threadIdx.y; tile < ntiles; tile += 8) ps += part[static_cast<size_t>(tile) * ldm + t];
+    for (int tile = threadIdx.y; tile < ntiles; tile += kRedRows) ps += part[static_cast<size_t>(tile) * ldm + t];
     red[threadIdx.y][threadIdx.x] = ps;
     __syncthreads();
     if (threadIdx.y != 0) return;
     double s = 0.0;
 #pragma unroll
-    for (int y = 0; y < 8; ++y) s += red[y][threadIdx.x];
+    for (int y = 0; y < kRedRows; ++y) s += red[y][threadIdx.x];
     const bool active = mdim[t] == 0;
     if (mode == 0) {
         out[t] = s;
