@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libmsgpu.so")
 
 SOURCES = ["msgpu_api.cu", "msgpu_batch.cu", "msgpu_dense.cu", "msgpu_host.cpp"]
 HEADERS = ["msgpu_device.cuh", "msgpu_kernels.cuh", "msgpu_resident.cuh", "msgpu_batch.cuh", "msgpu_dense.h", "msgpu_philox.h",
-           "msgpu_fused.cuh", "msgpu_spmm_tc.cuh"]
+           "msgpu_fused.cuh", "msgpu_spmm_tc.cuh", "msgpu_spmm_tm.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
