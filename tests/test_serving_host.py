@@ -204,3 +204,20 @@ def test_packs_shrink_to_the_budget():
     assert all(not r.error for r in res)
     assert eng.peak_reserved <= eng.budget
     assert all(len(p) <= 3 for p in eng.packs_seen)
+
+
+def test_pooled_batch_reservation_grows_with_a_larger_pack():
+    # one slot: a pack of two, then (arriving later) a pack of four on the same
+    # pooled batch; its reservation grows to the larger pack's footprint and is
+    # returned when the stream ends
+    first = [_small(i, arrival=0.0) for i in range(2)]
+    later = [_small(i, arrival=0.2) for i in range(2, 6)]
+    eng = FakePackEngine(hbm_budget=1 << 40, slots=1, work_s=0.05)
+    res = eng.serve(first + later, realtime=True)
+    assert all(not r.error for r in res)
+    assert eng.packs_seen == [[0, 1], [2, 3, 4, 5]]
+    assert len(eng.batches) == 1 and eng.batches[0].runs == 2 and eng.batches[0].closed
+    assert eng.contexts_created == 1 and eng.contexts_reused == 1
+    four = sum(SV.footprint(q.workload) for q in later)
+    assert eng.peak_reserved == max(four, sum(SV.footprint(q.workload) for q in first))
+    assert eng._reserved == 0
